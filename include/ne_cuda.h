@@ -1,0 +1,226 @@
+/*
+ * ne_cuda.h -- C-ABI of the B200 step() path of NativeEngine.
+ *
+ * The reference engine is a C++17 class API: ne::World::step()
+ * (src/world.hpp:138, src/world.cpp:133-146) called from ne::PhysicsWorld::step()
+ * (src/physics_world.hpp:217-246).  It has no C ABI and no device.  This header
+ * is the one boundary the B200 build adds underneath that API: the host facade
+ * (nativeengine_b200/host/include/ne/world.hpp) owns the bodies and calls these
+ * functions; bodies, contacts, islands and the warm-start cache live on the GPU.
+ *
+ * Conventions
+ *  - Plain C: POD structs, host pointers and sizes, no torch or CUDA types.
+ *  - Every function returns an int status (NE_OK == 0).  The reference has no
+ *    error channel (invalid handles are silent no-ops); device faults, capacity
+ *    exhaustion and unsupported features are reported here instead.
+ *  - One opaque NeWorld per world.  Each world owns one CUDA stream.  A world is
+ *    not thread-safe; distinct worlds may be used from distinct threads.
+ *  - Vectors are interleaved: x[3*i+0..2]; quaternions are (w,x,y,z) like ne::Q
+ *    (src/vmath.hpp:47-48).
+ *  - Features that the reference supports but this device path does not yet run
+ *    (joints, sleeping, CCD, triangle meshes, compounds) make ne_world_upload /
+ *    ne_world_step return NE_ERR_UNSUPPORTED.  There is no CPU fallback.
+ */
+#ifndef NE_CUDA_H
+#define NE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+    NE_OK = 0,
+    NE_ERR_ARG = 1,          /* bad pointer / size / enum value                  */
+    NE_ERR_CUDA = 2,         /* a CUDA runtime call failed                        */
+    NE_ERR_CAPACITY = 3,     /* a device capacity limit was hit and could not grow */
+    NE_ERR_UNSUPPORTED = 4,  /* feature not on the device path (see above)        */
+    NE_ERR_TIMEOUT = 5,      /* a bounded device wait ran out                     */
+    NE_ERR_NUMERIC = 6,      /* an iteration cap was hit (EPA face budget)        */
+    NE_ERR_NO_DEVICE = 7     /* no CUDA device visible                            */
+};
+
+/* ---- shapes: same tags and order as ne::Shape (src/body.hpp:24) ----------- */
+enum {
+    NE_SHAPE_SPHERE = 0,
+    NE_SHAPE_CYLINDER = 1,
+    NE_SHAPE_BOX = 2,
+    NE_SHAPE_CAPSULE = 3,
+    NE_SHAPE_CONVEX = 4,
+    NE_SHAPE_PLANE = 5,
+    NE_SHAPE_MESH = 6,
+    NE_SHAPE_COMPOUND = 7
+};
+
+/* ---- material combine modes: ne::World::Combine (src/world.hpp:85) ------- */
+enum {
+    NE_COMBINE_AVERAGE = 0,
+    NE_COMBINE_MIN = 1,
+    NE_COMBINE_MAX = 2,
+    NE_COMBINE_MULTIPLY = 3,
+    NE_COMBINE_GEOMETRIC_MEAN = 4
+};
+
+/* ---- per-body flag bits (ne::Body booleans, src/body.hpp:106-127) -------- */
+#define NE_BODY_DYNAMIC   1u
+#define NE_BODY_SLEEPING  2u
+#define NE_BODY_KINEMATIC 4u
+#define NE_BODY_SENSOR    8u
+#define NE_BODY_CCD      16u
+
+/* World configuration: the public fields of ne::World (src/world.hpp:75-136)
+ * that step() reads.  Joint counts are carried so that a world with joints
+ * is refused (NE_ERR_UNSUPPORTED) rather than silently stepped without them. */
+typedef struct NeWorldParams {
+    double half;                 /* Box::half (src/box.hpp:17)                  */
+    int32_t periodic;            /* Box::periodic                               */
+    int32_t open_boundary;       /* World::openBoundary                         */
+    double dt;                   /* World::dt                                   */
+    double restitution;          /* World::restitution                          */
+    double friction;             /* World::friction                             */
+    double contact_beta;         /* World::contactBeta                          */
+    double gravity[3];           /* World::gravity                              */
+    int32_t restitution_combine; /* World::restitutionCombine (NE_COMBINE_*)    */
+    int32_t friction_combine;    /* World::frictionCombine                      */
+    int32_t warm_start;          /* World::warmStart                            */
+    int32_t force_brute_force;   /* World::forceBruteForce                      */
+    int32_t capture_contacts;    /* World::captureContacts                      */
+    int32_t sleep_enabled;       /* World::sleepEnabled (must be 0 here)        */
+    double sleep_lin_vel, sleep_ang_vel, sleep_time, wake_vel;
+    uint32_t n_distance_joints;  /* World::distanceJoints.size() (must be 0)    */
+    uint32_t n_joints;           /* World::joints.size() (must be 0)            */
+} NeWorldParams;
+
+/* Fills p with ne::World's defaults (src/world.hpp:75-126, src/box.hpp:17-18). */
+void ne_world_params_default(NeWorldParams* p);
+
+/* Host-side body arrays (structure of arrays, n bodies).  Mirrors the fields of
+ * ne::Body (src/body.hpp:41-130) that step() reads or writes.  For upload every
+ * pointer except verts/nocollide (when unused) must be non-NULL; for download
+ * only the non-NULL state pointers are filled. */
+typedef struct NeBodyArrays {
+    uint32_t n;
+    /* dynamic state */
+    double* x;              /* [3n] centre of mass                           */
+    double* q;              /* [4n] orientation w,x,y,z (body -> world)      */
+    double* v;              /* [3n] linear velocity                          */
+    double* w;              /* [3n] angular velocity (world frame)           */
+    double* force;          /* [3n] force accumulator (cleared by step)      */
+    double* torque;         /* [3n] torque accumulator (cleared by step)     */
+    /* mass */
+    double* inv_mass;       /* [n]                                           */
+    double* inv_inertia;    /* [3n] diagonal of the body-frame inverse inertia */
+    /* shape */
+    int32_t* shape;         /* [n] NE_SHAPE_*                                */
+    double* radius;         /* [n]                                           */
+    double* half_height;    /* [n]                                           */
+    double* half_extents;   /* [3n] box half extents, or plane normal        */
+    uint32_t* vert_offset;  /* [n] first convex vertex in verts              */
+    uint32_t* vert_count;   /* [n] number of convex vertices                 */
+    double* verts;          /* [3*n_verts] body-frame convex vertices        */
+    uint32_t n_verts;
+    /* material, damping, gravity */
+    double* friction;       /* [n] (<0: inherit World::friction)             */
+    double* restitution;    /* [n] (<0: inherit World::restitution)          */
+    double* linear_damping; /* [n]                                           */
+    double* angular_damping;/* [n]                                           */
+    double* gravity_scale;  /* [n]                                           */
+    /* filtering */
+    uint32_t* layer;        /* [n]                                           */
+    uint32_t* mask;         /* [n]                                           */
+    uint32_t* flags;        /* [n] NE_BODY_* bits                            */
+    uint32_t* nocollide_offset; /* [n] into nocollide                        */
+    uint32_t* nocollide_count;  /* [n]                                       */
+    uint32_t* nocollide;    /* [n_nocollide] excluded partner indices         */
+    uint32_t n_nocollide;
+} NeBodyArrays;
+
+/* One resolved contact constraint of the last step, in solver order
+ * (sorted body pair, then slot) -- the device image of World::debugContacts
+ * (src/world.hpp:135-136, src/world.cpp:552) plus the converged impulses. */
+typedef struct NeContactArrays {
+    uint32_t* i;            /* [c] body index a (i < j)                      */
+    uint32_t* j;            /* [c] body index b                              */
+    uint32_t* slot;         /* [c] contact slot within the pair              */
+    double* point;          /* [3c] world contact point                      */
+    double* normal;         /* [3c] unit normal, b -> a                      */
+    double* depth;          /* [c] penetration                               */
+    double* n_imp;          /* [c] converged accumulated normal impulse      */
+    double* t_imp;          /* [c] accumulated friction impulse (scalar)     */
+} NeContactArrays;
+
+/* Per-step counters of the last successful step. */
+typedef struct NeStepStats {
+    uint64_t pairs;          /* broadphase candidate pairs (sorted, unique)   */
+    uint64_t survivors;      /* pairs passing filters + bounding-sphere cull  */
+    uint64_t contacts;       /* contact constraints                           */
+    uint64_t islands;        /* solver islands (connected components)         */
+    uint64_t max_island;     /* constraints in the largest island             */
+    uint64_t epa_cap_hits;   /* EPA runs that stopped at the 64-iteration cap */
+    uint64_t steps;          /* steps taken since upload                      */
+    uint64_t retries;        /* steps re-run after growing a device buffer    */
+} NeStepStats;
+
+typedef struct NeWorld NeWorld;
+
+/* Lifecycle.  Replaces constructing ne::World (src/world.hpp:73). */
+int ne_world_create(const NeWorldParams* params, NeWorld** out);
+int ne_world_destroy(NeWorld* world);
+/* Replaces assigning World's public config fields (src/world.hpp:75-136). */
+int ne_world_set_params(NeWorld* world, const NeWorldParams* params);
+
+/* Full (re)load of all bodies.  Replaces editing World::bodies
+ * (src/world.hpp:128) -- add/remove/setters in PhysicsWorld
+ * (src/physics_world.hpp:58-165,262-270) end here.  Does not clear the warm
+ * cache, matching the reference, whose cache survives body edits. */
+int ne_world_upload(NeWorld* world, const NeBodyArrays* bodies);
+/* Overwrite only x/q/v/w (each may be NULL to keep the device copy).  Same
+ * count as the last full upload. */
+int ne_world_upload_state(NeWorld* world, const double* x, const double* q,
+                          const double* v, const double* w);
+/* Copy the non-NULL state fields (x, q, v, w, force, torque) back to the host. */
+int ne_world_download(NeWorld* world, NeBodyArrays* out);
+
+/* Advance nsteps steps.  Replaces World::step() (src/world.cpp:133-146):
+ * integrate -> broadphase -> narrowphase -> constraint build + warm start ->
+ * 8 sequential-impulse iterations -> position correction -> warm-cache store ->
+ * wrap (periodic) or walls (reflective).  Synchronous: returns after the last
+ * step has finished on the device. */
+int ne_world_step(NeWorld* world, uint32_t nsteps);
+
+/* Replaces World::resetWarmCache() (src/world.hpp:140). */
+int ne_world_reset_warm_cache(NeWorld* world);
+
+/* Introspection of the last step (parity probes). */
+int ne_world_stats(const NeWorld* world, NeStepStats* out);
+/* Broadphase pairs of the last step, as World::broadphasePairs() returned them
+ * (src/world.cpp:424-501): sorted by (i, j), unique, i < j.  *count receives
+ * the total; at most cap pairs are written. */
+int ne_world_pairs(NeWorld* world, uint32_t* i, uint32_t* j, uint64_t cap,
+                   uint64_t* count);
+/* Contacts of the last step in solver order; *count receives the total. */
+int ne_world_contacts(NeWorld* world, NeContactArrays* out, uint64_t cap,
+                      uint64_t* count);
+/* Island partition of the last step: label[b] = smallest body index of the
+ * connected component of b over contacts whose two bodies both have
+ * invMass > 0 (the union-find of src/world.cpp:332-343 over islandPairs_);
+ * bodies in no such contact are their own label. */
+int ne_world_islands(NeWorld* world, uint32_t* label, uint32_t n);
+
+/* The CUDA stream the world launches on (as a void*; cast to cudaStream_t). */
+int ne_world_stream(const NeWorld* world, void** stream);
+/* Number of kernel launches made by the last ne_world_step call. */
+int ne_world_launch_count(const NeWorld* world, uint64_t* launches);
+
+/* Human-readable status / last CUDA error text. */
+const char* ne_status_string(int status);
+const char* ne_last_error(void);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif  /* NE_CUDA_H */

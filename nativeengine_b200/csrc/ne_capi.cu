@@ -1,0 +1,701 @@
+// ne_capi.cu -- the extern "C" boundary (include/ne_cuda.h): world lifecycle,
+// host <-> HBM packing of the body arrays, and the step loop with its
+// capacity retry.
+//
+// Capacities (pairs, surviving pairs, contacts) are data dependent.  Each step
+// is enqueued with the current capacities; the kernels never write past them
+// but raise ctl->abort and report the totals they needed.  The host then
+// restores the pre-step snapshot that k_integrate took, grows the buffers and
+// runs the step again -- so growth never changes the result, and steady-state
+// steps cost one small device->host read of the control block.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "ne_step.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_err(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define NE_CUDA_TRY(expr)                                                                         \
+    do {                                                                                          \
+        cudaError_t e_ = (expr);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return set_err(NE_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+template <typename T>
+int dalloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) return set_err(NE_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return NE_OK;
+}
+
+template <typename T>
+void dfree(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+inline size_t grow_to(uint64_t need) { return (size_t)(need + need / 4 + 1024); }
+
+}  // namespace
+
+struct NeWorld {
+    NeWorldParams p{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t n = 0;
+    neb::DevWorld d{};
+    neb::Ctl* h_ctl = nullptr;   // pinned mirror of d.ctl
+    // broadphase constants
+    double max_r = 0.0, cell = 0.0;
+    long long nc[3] = {1, 1, 1};
+    int brute = 1;
+    uint32_t nplanes = 0;
+    int key_bits = 64;
+    // capacities (entries)
+    uint64_t Pcap = 0, Scap = 0, Ccap = 0;
+    size_t nverts_alloc = 0, nnc_alloc = 0, nplanes_alloc = 0;
+    std::vector<double> h_invmass;   // for upload_state packing
+    std::vector<neb::D4> stage;      // host packing buffer
+    NeStepStats stats{};
+    uint64_t launches = 0;
+    bool has_bodies = false;
+};
+
+namespace {
+
+void free_body_arrays(NeWorld* w) {
+    neb::DevWorld& d = w->d;
+    dfree(d.pos); dfree(d.quat); dfree(d.vel); dfree(d.omg); dfree(d.frc); dfree(d.trq);
+    dfree(d.inert); dfree(d.geom); dfree(d.ext); dfree(d.mat); dfree(d.meta); dfree(d.vrng); dfree(d.ncrng);
+    dfree(d.s_pos); dfree(d.s_quat); dfree(d.s_vel); dfree(d.s_omg); dfree(d.s_frc); dfree(d.s_trq);
+    dfree(d.key[0]); dfree(d.key[1]); dfree(d.val[0]); dfree(d.val[1]);
+    dfree(d.bcnt); dfree(d.boff); dfree(d.parent);
+}
+
+void free_pair_arrays(NeWorld* w) {
+    neb::DevWorld& d = w->d;
+    dfree(d.pair_i); dfree(d.pair_j); dfree(d.pflag); dfree(d.poff);
+}
+
+void free_surv_arrays(NeWorld* w) {
+    neb::DevWorld& d = w->d;
+    dfree(d.surv); dfree(d.ccnt); dfree(d.coff); dfree(d.cn); dfree(d.cp);
+}
+
+void free_con_arrays(NeWorld* w) {
+    neb::DevWorld& d = w->d;
+    dfree(d.ci); dfree(d.cj); dfree(d.cslot); dfree(d.con_n); dfree(d.con_ra); dfree(d.con_rb); dfree(d.con_p);
+    dfree(d.con_imp); dfree(d.ilab[0]); dfree(d.ilab[1]); dfree(d.iord[0]); dfree(d.iord[1]); dfree(d.iflag);
+    dfree(d.ioff); dfree(d.istart);
+}
+
+int alloc_scratch(NeWorld* w) {
+    neb::DevWorld& d = w->d;
+    dfree(d.hist);
+    dfree(d.tsum);
+    uint64_t sortn = std::max<uint64_t>(w->n, w->Ccap);
+    size_t hw = neb::radix_hist_words((uint32_t)sortn);
+    uint64_t scann = std::max<uint64_t>(std::max<uint64_t>(w->Pcap, w->Scap), std::max<uint64_t>(hw, sortn));
+    int rc;
+    if ((rc = dalloc(&d.hist, hw)) != NE_OK) return rc;
+    if ((rc = dalloc(&d.tsum, neb::scan_tsum_words((uint32_t)scann) + 8)) != NE_OK) return rc;
+    return NE_OK;
+}
+
+int alloc_pairs(NeWorld* w, uint64_t cap) {
+    free_pair_arrays(w);
+    neb::DevWorld& d = w->d;
+    int rc;
+    if ((rc = dalloc(&d.pair_i, cap)) || (rc = dalloc(&d.pair_j, cap)) || (rc = dalloc(&d.pflag, cap)) ||
+        (rc = dalloc(&d.poff, cap)))
+        return rc;
+    w->Pcap = cap;
+    return NE_OK;
+}
+
+int alloc_surv(NeWorld* w, uint64_t cap) {
+    free_surv_arrays(w);
+    neb::DevWorld& d = w->d;
+    int rc;
+    if ((rc = dalloc(&d.surv, cap)) || (rc = dalloc(&d.ccnt, cap)) || (rc = dalloc(&d.coff, cap)) ||
+        (rc = dalloc(&d.cn, 4 * cap)) || (rc = dalloc(&d.cp, 4 * cap)))
+        return rc;
+    w->Scap = cap;
+    return NE_OK;
+}
+
+// Contact-sized arrays.  The warm cache survives a resize: the buffer holding
+// the previous step is copied into the new allocation.
+int alloc_cons(NeWorld* w, uint64_t cap) {
+    neb::DevWorld& d = w->d;
+    free_con_arrays(w);
+    int rc;
+    if ((rc = dalloc(&d.ci, cap)) || (rc = dalloc(&d.cj, cap)) || (rc = dalloc(&d.cslot, cap)) ||
+        (rc = dalloc(&d.con_n, cap)) || (rc = dalloc(&d.con_ra, cap)) || (rc = dalloc(&d.con_rb, cap)) ||
+        (rc = dalloc(&d.con_p, cap)) || (rc = dalloc(&d.con_imp, cap)) || (rc = dalloc(&d.ilab[0], cap)) ||
+        (rc = dalloc(&d.ilab[1], cap)) || (rc = dalloc(&d.iord[0], cap)) || (rc = dalloc(&d.iord[1], cap)) ||
+        (rc = dalloc(&d.iflag, cap)) || (rc = dalloc(&d.ioff, cap)) || (rc = dalloc(&d.istart, cap + 1)))
+        return rc;
+    unsigned long long* nk[2] = {nullptr, nullptr};
+    double* ni[2] = {nullptr, nullptr};
+    for (int b = 0; b < 2; ++b) {
+        if ((rc = dalloc(&nk[b], cap)) || (rc = dalloc(&ni[b], cap))) return rc;
+    }
+    if (d.wkey[0]) {
+        NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+        NE_CUDA_TRY(cudaMemcpy(w->h_ctl, d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost));
+        const uint32_t ws = w->h_ctl->wsel;
+        const uint64_t cnt = std::min<uint64_t>(w->h_ctl->wcount[ws], cap);
+        if (cnt) {
+            NE_CUDA_TRY(cudaMemcpy(nk[ws], d.wkey[ws], cnt * sizeof(unsigned long long), cudaMemcpyDeviceToDevice));
+            NE_CUDA_TRY(cudaMemcpy(ni[ws], d.wimp[ws], cnt * sizeof(double), cudaMemcpyDeviceToDevice));
+        }
+    }
+    for (int b = 0; b < 2; ++b) {
+        dfree(d.wkey[b]);
+        dfree(d.wimp[b]);
+        d.wkey[b] = nk[b];
+        d.wimp[b] = ni[b];
+    }
+    w->Ccap = cap;
+    return NE_OK;
+}
+
+neb::StepArgs make_args(const NeWorld* w) {
+    neb::StepArgs a;
+    a.d = w->d;
+    a.n = w->n;
+    a.dom.half = w->p.half;
+    a.dom.periodic = w->p.periodic ? 1 : 0;
+    a.dt = w->p.dt;
+    a.restitution = w->p.restitution;
+    a.friction = w->p.friction;
+    a.beta = w->p.contact_beta;
+    a.g = neb::mk(w->p.gravity[0], w->p.gravity[1], w->p.gravity[2]);
+    a.rcomb = w->p.restitution_combine;
+    a.fcomb = w->p.friction_combine;
+    a.warm = w->p.warm_start ? 1 : 0;
+    a.open_boundary = w->p.open_boundary ? 1 : 0;
+    a.cell = w->cell;
+    for (int k = 0; k < 3; ++k) a.nc[k] = w->nc[k];
+    a.brute = w->brute;
+    a.nplanes = w->nplanes;
+    a.key_bits = w->key_bits;
+    a.Pcap = w->Pcap;
+    a.Scap = w->Scap;
+    a.Ccap = w->Ccap;
+    return a;
+}
+
+int check_params(const NeWorldParams* p) {
+    if (!p) return set_err(NE_ERR_ARG, "params is NULL");
+    if (p->restitution_combine < 0 || p->restitution_combine > 4 || p->friction_combine < 0 || p->friction_combine > 4)
+        return set_err(NE_ERR_ARG, "combine mode out of range");
+    if (p->sleep_enabled) return set_err(NE_ERR_UNSUPPORTED, "sleeping is not on the device path");
+    if (p->n_distance_joints || p->n_joints) return set_err(NE_ERR_UNSUPPORTED, "joints are not on the device path");
+    return NE_OK;
+}
+
+// Broadphase constants of World::broadphasePairs() (src/world.cpp:427-457):
+// cell = 2 * max bounding radius over grid bodies, brute force below 64
+// bodies, periodic cell counts nc = max(1, floor(L / cell)).
+void derive_grid(NeWorld* w, const std::vector<double>& boundR, const std::vector<int>& shape) {
+    double maxR = 0.0;
+    w->nplanes = 0;
+    for (uint32_t i = 0; i < w->n; ++i) {
+        if (shape[i] == NE_SHAPE_PLANE || shape[i] == NE_SHAPE_MESH) { ++w->nplanes; continue; }
+        maxR = (maxR < boundR[i]) ? boundR[i] : maxR;
+    }
+    w->max_r = maxR;
+    w->cell = 2.0 * maxR;
+    w->brute = (w->p.force_brute_force || w->n < 64 || w->cell < 1e-9) ? 1 : 0;
+    w->nc[0] = w->nc[1] = w->nc[2] = 1;
+    if (w->p.periodic && !w->brute) {
+        const double L = 2.0 * w->p.half;
+        for (int a = 0; a < 3; ++a) {
+            long long m = (long long)(int)std::floor(L / w->cell);
+            w->nc[a] = m < 1 ? 1 : m;
+        }
+    }
+    if (w->p.periodic) {
+        int bits = 0;
+        for (int a = 0; a < 3; ++a) {
+            long long m = w->nc[a];
+            int b = 0;
+            if (m > (1ll << 21)) b = 21;
+            else while ((1ll << b) < m) ++b;
+            bits += b;
+        }
+        w->key_bits = ((bits + 1 + 7) / 8) * 8;
+    } else {
+        w->key_bits = 64;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void ne_world_params_default(NeWorldParams* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->half = 12.0;
+    p->periodic = 0;
+    p->open_boundary = 0;
+    p->dt = 1.0 / 120.0;
+    p->restitution = 1.0;
+    p->friction = 0.0;
+    p->contact_beta = 0.2;
+    p->restitution_combine = NE_COMBINE_MAX;
+    p->friction_combine = NE_COMBINE_GEOMETRIC_MEAN;
+    p->warm_start = 1;
+    p->force_brute_force = 0;
+    p->capture_contacts = 0;
+    p->sleep_enabled = 0;
+    p->sleep_lin_vel = 0.05;
+    p->sleep_ang_vel = 0.05;
+    p->sleep_time = 0.5;
+    p->wake_vel = 0.5;
+}
+
+const char* ne_status_string(int s) {
+    switch (s) {
+        case NE_OK: return "ok";
+        case NE_ERR_ARG: return "invalid argument";
+        case NE_ERR_CUDA: return "CUDA error";
+        case NE_ERR_CAPACITY: return "device capacity exceeded";
+        case NE_ERR_UNSUPPORTED: return "feature not supported on the device path";
+        case NE_ERR_TIMEOUT: return "device wait timed out";
+        case NE_ERR_NUMERIC: return "narrowphase budget exceeded";
+        case NE_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+const char* ne_last_error(void) { return g_last_error.c_str(); }
+
+int ne_world_create(const NeWorldParams* params, NeWorld** out) {
+    if (!out) return set_err(NE_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int rc = check_params(params);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return set_err(NE_ERR_NO_DEVICE, "no CUDA device");
+    NeWorld* w = new NeWorld();
+    w->p = *params;
+    NE_CUDA_TRY(cudaGetDevice(&w->device));
+    NE_CUDA_TRY(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+    NE_CUDA_TRY(cudaMallocHost((void**)&w->h_ctl, sizeof(neb::Ctl)));
+    if ((rc = dalloc(&w->d.ctl, 1))) { ne_world_destroy(w); return rc; }
+    std::memset(w->h_ctl, 0, sizeof(neb::Ctl));
+    NE_CUDA_TRY(cudaMemcpy(w->d.ctl, w->h_ctl, sizeof(neb::Ctl), cudaMemcpyHostToDevice));
+    *out = w;
+    return NE_OK;
+}
+
+int ne_world_destroy(NeWorld* w) {
+    if (!w) return NE_OK;
+    if (w->stream) cudaStreamSynchronize(w->stream);
+    free_body_arrays(w);
+    free_pair_arrays(w);
+    free_surv_arrays(w);
+    free_con_arrays(w);
+    neb::DevWorld& d = w->d;
+    dfree(d.verts); dfree(d.nc); dfree(d.planes);
+    for (int b = 0; b < 2; ++b) { dfree(d.wkey[b]); dfree(d.wimp[b]); }
+    dfree(d.hist); dfree(d.tsum); dfree(d.ctl);
+    if (w->h_ctl) cudaFreeHost(w->h_ctl);
+    if (w->stream) cudaStreamDestroy(w->stream);
+    delete w;
+    return NE_OK;
+}
+
+int ne_world_set_params(NeWorld* w, const NeWorldParams* params) {
+    if (!w) return set_err(NE_ERR_ARG, "world is NULL");
+    int rc = check_params(params);
+    if (rc) return rc;
+    const bool regrid = params->half != w->p.half || params->periodic != w->p.periodic ||
+                        params->force_brute_force != w->p.force_brute_force;
+    w->p = *params;
+    if (regrid && w->has_bodies) {
+        // Recompute the grid constants from the device copy of the shapes.
+        std::vector<neb::D4> inert(w->n);
+        std::vector<uint4> meta(w->n);
+        NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+        NE_CUDA_TRY(cudaMemcpy(inert.data(), w->d.inert, w->n * sizeof(neb::D4), cudaMemcpyDeviceToHost));
+        NE_CUDA_TRY(cudaMemcpy(meta.data(), w->d.meta, w->n * sizeof(uint4), cudaMemcpyDeviceToHost));
+        std::vector<double> r(w->n);
+        std::vector<int> s(w->n);
+        for (uint32_t i = 0; i < w->n; ++i) { r[i] = inert[i].w; s[i] = (int)meta[i].x; }
+        derive_grid(w, r, s);
+    }
+    return NE_OK;
+}
+
+int ne_world_upload(NeWorld* w, const NeBodyArrays* b) {
+    if (!w || !b) return set_err(NE_ERR_ARG, "NULL argument");
+    const uint32_t n = b->n;
+    if (n > (1u << 24)) return set_err(NE_ERR_CAPACITY, "more than 2^24 bodies");
+    if (n && (!b->x || !b->q || !b->v || !b->w || !b->inv_mass || !b->inv_inertia || !b->shape || !b->radius ||
+              !b->half_height || !b->half_extents || !b->friction || !b->restitution || !b->linear_damping ||
+              !b->angular_damping || !b->gravity_scale || !b->layer || !b->mask || !b->flags))
+        return set_err(NE_ERR_ARG, "a required body array is NULL");
+    for (uint32_t i = 0; i < n; ++i) {
+        const int s = b->shape[i];
+        if (s < 0 || s > NE_SHAPE_COMPOUND) return set_err(NE_ERR_ARG, "shape tag out of range");
+        if (s == NE_SHAPE_MESH || s == NE_SHAPE_COMPOUND)
+            return set_err(NE_ERR_UNSUPPORTED, "triangle meshes and compounds are not on the device path");
+        if (s == NE_SHAPE_CONVEX) {
+            if (!b->verts || !b->vert_offset || !b->vert_count) return set_err(NE_ERR_ARG, "convex body without vertices");
+            if ((uint64_t)b->vert_offset[i] + b->vert_count[i] > b->n_verts)
+                return set_err(NE_ERR_ARG, "convex vertex range out of bounds");
+        }
+        if ((b->flags[i] & NE_BODY_CCD) && b->inv_mass[i] > 0.0 && !(b->flags[i] & NE_BODY_SLEEPING))
+            return set_err(NE_ERR_UNSUPPORTED, "continuous collision is not on the device path");
+        if (b->nocollide_count && b->nocollide_count[i]) {
+            if (!b->nocollide || !b->nocollide_offset ||
+                (uint64_t)b->nocollide_offset[i] + b->nocollide_count[i] > b->n_nocollide)
+                return set_err(NE_ERR_ARG, "noCollide range out of bounds");
+        }
+    }
+    NE_CUDA_TRY(cudaSetDevice(w->device));
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    int rc;
+    neb::DevWorld& d = w->d;
+    if (n != w->n || !d.pos) {
+        free_body_arrays(w);
+        w->n = n;
+        const size_t m = n ? n : 1;
+        if ((rc = dalloc(&d.pos, m)) || (rc = dalloc(&d.quat, m)) || (rc = dalloc(&d.vel, m)) ||
+            (rc = dalloc(&d.omg, m)) || (rc = dalloc(&d.frc, m)) || (rc = dalloc(&d.trq, m)) ||
+            (rc = dalloc(&d.inert, m)) || (rc = dalloc(&d.geom, m)) || (rc = dalloc(&d.ext, m)) ||
+            (rc = dalloc(&d.mat, m)) || (rc = dalloc(&d.meta, m)) || (rc = dalloc(&d.vrng, m)) ||
+            (rc = dalloc(&d.ncrng, m)) || (rc = dalloc(&d.s_pos, m)) || (rc = dalloc(&d.s_quat, m)) ||
+            (rc = dalloc(&d.s_vel, m)) || (rc = dalloc(&d.s_omg, m)) || (rc = dalloc(&d.s_frc, m)) ||
+            (rc = dalloc(&d.s_trq, m)) || (rc = dalloc(&d.key[0], m)) || (rc = dalloc(&d.key[1], m)) ||
+            (rc = dalloc(&d.val[0], m)) || (rc = dalloc(&d.val[1], m)) || (rc = dalloc(&d.bcnt, m)) ||
+            (rc = dalloc(&d.boff, m)) || (rc = dalloc(&d.parent, m)))
+            return rc;
+    }
+    // Pack the host arrays into the 32-byte device records.
+    std::vector<neb::D4>& st = w->stage;
+    st.assign(n ? n : 1, neb::D4{0, 0, 0, 0});
+    auto put = [&](neb::D4* dst) -> int {
+        if (!n) return NE_OK;
+        cudaError_t e = cudaMemcpy(dst, st.data(), n * sizeof(neb::D4), cudaMemcpyHostToDevice);
+        return e == cudaSuccess ? NE_OK : set_err(NE_ERR_CUDA, cudaGetErrorString(e));
+    };
+    auto v3 = [&](const double* a, uint32_t i, double wv) { return neb::D4{a[3 * i], a[3 * i + 1], a[3 * i + 2], wv}; };
+    w->h_invmass.assign(b->inv_mass, b->inv_mass + n);
+    for (uint32_t i = 0; i < n; ++i) st[i] = v3(b->x, i, b->inv_mass[i]);
+    if ((rc = put(d.pos))) return rc;
+    for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{b->q[4 * i], b->q[4 * i + 1], b->q[4 * i + 2], b->q[4 * i + 3]};
+    if ((rc = put(d.quat))) return rc;
+    for (uint32_t i = 0; i < n; ++i) st[i] = v3(b->v, i, 0.0);
+    if ((rc = put(d.vel))) return rc;
+    for (uint32_t i = 0; i < n; ++i) st[i] = v3(b->w, i, 0.0);
+    if ((rc = put(d.omg))) return rc;
+    for (uint32_t i = 0; i < n; ++i) st[i] = b->force ? v3(b->force, i, 0.0) : neb::D4{0, 0, 0, 0};
+    if ((rc = put(d.frc))) return rc;
+    for (uint32_t i = 0; i < n; ++i) st[i] = b->torque ? v3(b->torque, i, 0.0) : neb::D4{0, 0, 0, 0};
+    if ((rc = put(d.trq))) return rc;
+
+    // Convex vertex pool (needed for bounding radii below).
+    std::vector<neb::D4> verts(b->n_verts ? b->n_verts : 1);
+    for (uint32_t k = 0; k < b->n_verts; ++k) verts[k] = v3(b->verts, k, 0.0);
+    dfree(d.verts);
+    if ((rc = dalloc(&d.verts, verts.size()))) return rc;
+    NE_CUDA_TRY(cudaMemcpy(d.verts, verts.data(), verts.size() * sizeof(neb::D4), cudaMemcpyHostToDevice));
+
+    std::vector<double> boundR(n);
+    std::vector<int> shapes(n);
+    std::vector<uint32_t> planes;
+    for (uint32_t i = 0; i < n; ++i) {
+        const int s = b->shape[i];
+        shapes[i] = s;
+        const neb::V3 he = neb::mk(b->half_extents[3 * i], b->half_extents[3 * i + 1], b->half_extents[3 * i + 2]);
+        const neb::D4* vp = (s == NE_SHAPE_CONVEX) ? verts.data() + b->vert_offset[i] : verts.data();
+        const int nv = (s == NE_SHAPE_CONVEX) ? (int)b->vert_count[i] : 0;
+        boundR[i] = neb::bounding_radius(s, b->radius[i], b->half_height[i], he, vp, nv);
+        if (s == NE_SHAPE_PLANE || s == NE_SHAPE_MESH) planes.push_back(i);
+        st[i] = v3(b->inv_inertia, i, boundR[i]);
+    }
+    if ((rc = put(d.inert))) return rc;
+    for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{b->radius[i], b->half_height[i], b->gravity_scale[i], 0.0};
+    if ((rc = put(d.geom))) return rc;
+    for (uint32_t i = 0; i < n; ++i) st[i] = v3(b->half_extents, i, 0.0);
+    if ((rc = put(d.ext))) return rc;
+    for (uint32_t i = 0; i < n; ++i)
+        st[i] = neb::D4{b->friction[i], b->restitution[i], b->linear_damping[i], b->angular_damping[i]};
+    if ((rc = put(d.mat))) return rc;
+
+    std::vector<uint4> meta(n ? n : 1);
+    std::vector<uint2> vr(n ? n : 1), ncr(n ? n : 1);
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t fl = b->flags[i] & 0xFFFFu;
+        const bool mut = b->inv_mass[i] > 0.0 || b->inv_inertia[3 * i] != 0.0 || b->inv_inertia[3 * i + 1] != 0.0 ||
+                         b->inv_inertia[3 * i + 2] != 0.0;
+        if (mut) fl |= neb::kFlagMutable;
+        meta[i] = make_uint4((uint32_t)b->shape[i], fl, b->layer[i], b->mask[i]);
+        vr[i] = (b->shape[i] == NE_SHAPE_CONVEX) ? make_uint2(b->vert_offset[i], b->vert_count[i]) : make_uint2(0, 0);
+        ncr[i] = (b->nocollide_count && b->nocollide_count[i])
+                     ? make_uint2(b->nocollide_offset[i], b->nocollide_count[i])
+                     : make_uint2(0, 0);
+    }
+    if (n) {
+        NE_CUDA_TRY(cudaMemcpy(d.meta, meta.data(), n * sizeof(uint4), cudaMemcpyHostToDevice));
+        NE_CUDA_TRY(cudaMemcpy(d.vrng, vr.data(), n * sizeof(uint2), cudaMemcpyHostToDevice));
+        NE_CUDA_TRY(cudaMemcpy(d.ncrng, ncr.data(), n * sizeof(uint2), cudaMemcpyHostToDevice));
+    }
+    dfree(d.nc);
+    if ((rc = dalloc(&d.nc, b->n_nocollide ? b->n_nocollide : 1))) return rc;
+    if (b->n_nocollide && b->nocollide)
+        NE_CUDA_TRY(cudaMemcpy(d.nc, b->nocollide, b->n_nocollide * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    dfree(d.planes);
+    if ((rc = dalloc(&d.planes, planes.size() ? planes.size() : 1))) return rc;
+    if (!planes.empty())
+        NE_CUDA_TRY(cudaMemcpy(d.planes, planes.data(), planes.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+
+    derive_grid(w, boundR, shapes);
+
+    // Initial capacities; they grow on demand (see ne_world_step).
+    if (!w->Pcap) {
+        if ((rc = alloc_pairs(w, std::max<uint64_t>(16ull * n, 4096)))) return rc;
+        if ((rc = alloc_surv(w, std::max<uint64_t>(4ull * n, 1024)))) return rc;
+        if ((rc = alloc_cons(w, std::max<uint64_t>(4ull * n, 1024)))) return rc;
+    }
+    if ((rc = alloc_scratch(w))) return rc;
+    w->has_bodies = true;
+    std::memset(&w->stats, 0, sizeof(w->stats));
+    return NE_OK;
+}
+
+int ne_world_upload_state(NeWorld* w, const double* x, const double* q, const double* v, const double* wv) {
+    if (!w || !w->has_bodies) return set_err(NE_ERR_ARG, "world has no bodies");
+    const uint32_t n = w->n;
+    if (!n) return NE_OK;
+    std::vector<neb::D4>& st = w->stage;
+    st.resize(n);
+    auto put = [&](neb::D4* dst) -> int {
+        cudaError_t e = cudaMemcpyAsync(dst, st.data(), n * sizeof(neb::D4), cudaMemcpyHostToDevice, w->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+        return e == cudaSuccess ? NE_OK : set_err(NE_ERR_CUDA, cudaGetErrorString(e));
+    };
+    int rc;
+    if (x) {
+        for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{x[3 * i], x[3 * i + 1], x[3 * i + 2], w->h_invmass[i]};
+        if ((rc = put(w->d.pos))) return rc;
+    }
+    if (q) {
+        for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]};
+        if ((rc = put(w->d.quat))) return rc;
+    }
+    if (v) {
+        for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0};
+        if ((rc = put(w->d.vel))) return rc;
+    }
+    if (wv) {
+        for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{wv[3 * i], wv[3 * i + 1], wv[3 * i + 2], 0.0};
+        if ((rc = put(w->d.omg))) return rc;
+    }
+    return NE_OK;
+}
+
+int ne_world_download(NeWorld* w, NeBodyArrays* out) {
+    if (!w || !out) return set_err(NE_ERR_ARG, "NULL argument");
+    if (!w->has_bodies) return set_err(NE_ERR_ARG, "world has no bodies");
+    const uint32_t n = std::min(w->n, out->n);
+    if (!n) return NE_OK;
+    std::vector<neb::D4>& st = w->stage;
+    st.resize(w->n);
+    auto get = [&](const neb::D4* src) -> int {
+        cudaError_t e = cudaMemcpyAsync(st.data(), src, n * sizeof(neb::D4), cudaMemcpyDeviceToHost, w->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+        return e == cudaSuccess ? NE_OK : set_err(NE_ERR_CUDA, cudaGetErrorString(e));
+    };
+    int rc;
+    auto unpack3 = [&](double* dst) {
+        for (uint32_t i = 0; i < n; ++i) { dst[3 * i] = st[i].x; dst[3 * i + 1] = st[i].y; dst[3 * i + 2] = st[i].z; }
+    };
+    if (out->x) { if ((rc = get(w->d.pos))) return rc; unpack3(out->x); }
+    if (out->q) {
+        if ((rc = get(w->d.quat))) return rc;
+        for (uint32_t i = 0; i < n; ++i) {
+            out->q[4 * i] = st[i].x; out->q[4 * i + 1] = st[i].y; out->q[4 * i + 2] = st[i].z; out->q[4 * i + 3] = st[i].w;
+        }
+    }
+    if (out->v) { if ((rc = get(w->d.vel))) return rc; unpack3(out->v); }
+    if (out->w) { if ((rc = get(w->d.omg))) return rc; unpack3(out->w); }
+    if (out->force) { if ((rc = get(w->d.frc))) return rc; unpack3(out->force); }
+    if (out->torque) { if ((rc = get(w->d.trq))) return rc; unpack3(out->torque); }
+    return NE_OK;
+}
+
+int ne_world_step(NeWorld* w, uint32_t nsteps) {
+    if (!w) return set_err(NE_ERR_ARG, "world is NULL");
+    if (!w->has_bodies) return set_err(NE_ERR_ARG, "world has no bodies");
+    NE_CUDA_TRY(cudaSetDevice(w->device));
+    w->launches = 0;
+    int status = NE_OK;
+    if (w->n == 0) { w->stats.steps += nsteps; return NE_OK; }
+    for (uint32_t s = 0; s < nsteps; ++s) {
+        for (int attempt = 0;; ++attempt) {
+            if (attempt > 16) return set_err(NE_ERR_CAPACITY, "step did not fit after repeated growth");
+            neb::StepArgs a = make_args(w);
+            neb::launch_step(a, w->stream, &w->launches);
+            NE_CUDA_TRY(cudaGetLastError());
+            NE_CUDA_TRY(cudaMemcpyAsync(w->h_ctl, w->d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost, w->stream));
+            NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+            const neb::Ctl& c = *w->h_ctl;
+            if (!c.abort) break;
+            // Restore the pre-step state and grow whatever overflowed.
+            const size_t bytes = (size_t)w->n * sizeof(neb::D4);
+            neb::DevWorld& d = w->d;
+            NE_CUDA_TRY(cudaMemcpyAsync(d.pos, d.s_pos, bytes, cudaMemcpyDeviceToDevice, w->stream));
+            NE_CUDA_TRY(cudaMemcpyAsync(d.quat, d.s_quat, bytes, cudaMemcpyDeviceToDevice, w->stream));
+            NE_CUDA_TRY(cudaMemcpyAsync(d.vel, d.s_vel, bytes, cudaMemcpyDeviceToDevice, w->stream));
+            NE_CUDA_TRY(cudaMemcpyAsync(d.omg, d.s_omg, bytes, cudaMemcpyDeviceToDevice, w->stream));
+            NE_CUDA_TRY(cudaMemcpyAsync(d.frc, d.s_frc, bytes, cudaMemcpyDeviceToDevice, w->stream));
+            NE_CUDA_TRY(cudaMemcpyAsync(d.trq, d.s_trq, bytes, cudaMemcpyDeviceToDevice, w->stream));
+            NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+            int rc = NE_OK;
+            bool grew = false;
+            if ((int)c.need_bits > w->key_bits) {
+                w->key_bits = (((int)c.need_bits + 7) / 8) * 8;
+                grew = true;
+            }
+            if (c.P > w->Pcap) {
+                if (c.P > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 candidate pairs");
+                if ((rc = alloc_pairs(w, grow_to(c.P)))) return rc;
+                grew = true;
+            } else if (c.S > w->Scap) {
+                if ((rc = alloc_surv(w, grow_to(c.S)))) return rc;
+                grew = true;
+            } else if (c.C > w->Ccap) {
+                if (c.C > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 contacts");
+                if ((rc = alloc_cons(w, grow_to(c.C)))) return rc;
+                grew = true;
+            }
+            if (!grew) return set_err(NE_ERR_CAPACITY, "step aborted without a growable cause");
+            if ((rc = alloc_scratch(w))) return rc;
+            ++w->stats.retries;
+        }
+        const neb::Ctl& c = *w->h_ctl;
+        // Shrink the cell-key sort to the bits this step needed.
+        if (!w->p.periodic) {
+            int kb = (((int)c.need_bits + 7) / 8) * 8;
+            if (kb >= 8) w->key_bits = kb;
+        }
+        w->stats.pairs = c.P;
+        w->stats.survivors = c.S;
+        w->stats.contacts = c.C;
+        w->stats.islands = c.islands;
+        w->stats.max_island = c.max_island;
+        w->stats.epa_cap_hits += c.epa_cap_hits;
+        w->stats.steps += 1;
+        if (c.flags & 1u) status = set_err(NE_ERR_NUMERIC, "an EPA or clipping budget was exceeded");
+    }
+    return status;
+}
+
+int ne_world_reset_warm_cache(NeWorld* w) {
+    if (!w) return set_err(NE_ERR_ARG, "world is NULL");
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    NE_CUDA_TRY(cudaMemcpy(w->h_ctl, w->d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost));
+    w->h_ctl->wcount[0] = w->h_ctl->wcount[1] = 0;
+    NE_CUDA_TRY(cudaMemcpy(w->d.ctl, w->h_ctl, sizeof(neb::Ctl), cudaMemcpyHostToDevice));
+    return NE_OK;
+}
+
+int ne_world_stats(const NeWorld* w, NeStepStats* out) {
+    if (!w || !out) return set_err(NE_ERR_ARG, "NULL argument");
+    *out = w->stats;
+    return NE_OK;
+}
+
+int ne_world_pairs(NeWorld* w, uint32_t* pi, uint32_t* pj, uint64_t cap, uint64_t* count) {
+    if (!w || !count) return set_err(NE_ERR_ARG, "NULL argument");
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    const uint64_t P = w->stats.pairs;
+    *count = P;
+    const uint64_t m = std::min(P, cap);
+    if (m && pi) NE_CUDA_TRY(cudaMemcpy(pi, w->d.pair_i, m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (m && pj) NE_CUDA_TRY(cudaMemcpy(pj, w->d.pair_j, m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    return NE_OK;
+}
+
+int ne_world_contacts(NeWorld* w, NeContactArrays* out, uint64_t cap, uint64_t* count) {
+    if (!w || !out || !count) return set_err(NE_ERR_ARG, "NULL argument");
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    const uint64_t C = w->stats.contacts;
+    *count = C;
+    const uint64_t m = std::min(C, cap);
+    if (!m) return NE_OK;
+    neb::DevWorld& d = w->d;
+    if (out->i) NE_CUDA_TRY(cudaMemcpy(out->i, d.ci, m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (out->j) NE_CUDA_TRY(cudaMemcpy(out->j, d.cj, m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (out->slot) NE_CUDA_TRY(cudaMemcpy(out->slot, d.cslot, m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    std::vector<neb::D4> t(m);
+    if (out->point) {
+        NE_CUDA_TRY(cudaMemcpy(t.data(), d.con_p, m * sizeof(neb::D4), cudaMemcpyDeviceToHost));
+        for (uint64_t k = 0; k < m; ++k) { out->point[3 * k] = t[k].x; out->point[3 * k + 1] = t[k].y; out->point[3 * k + 2] = t[k].z; }
+    }
+    if (out->normal || out->depth) {
+        NE_CUDA_TRY(cudaMemcpy(t.data(), d.con_n, m * sizeof(neb::D4), cudaMemcpyDeviceToHost));
+        for (uint64_t k = 0; k < m; ++k) {
+            if (out->normal) { out->normal[3 * k] = t[k].x; out->normal[3 * k + 1] = t[k].y; out->normal[3 * k + 2] = t[k].z; }
+            if (out->depth) out->depth[k] = t[k].w;
+        }
+    }
+    if (out->n_imp || out->t_imp) {
+        std::vector<double2> imp(m);
+        NE_CUDA_TRY(cudaMemcpy(imp.data(), d.con_imp, m * sizeof(double2), cudaMemcpyDeviceToHost));
+        for (uint64_t k = 0; k < m; ++k) {
+            if (out->n_imp) out->n_imp[k] = imp[k].x;
+            if (out->t_imp) out->t_imp[k] = imp[k].y;
+        }
+    }
+    return NE_OK;
+}
+
+int ne_world_islands(NeWorld* w, uint32_t* label, uint32_t n) {
+    if (!w || !label) return set_err(NE_ERR_ARG, "NULL argument");
+    if (n > w->n) return set_err(NE_ERR_ARG, "n exceeds the body count");
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    std::vector<uint32_t> parent(w->n);
+    if (w->n) NE_CUDA_TRY(cudaMemcpy(parent.data(), w->d.parent, w->n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t x = i;
+        for (uint32_t guard = 0; parent[x] != x && guard < w->n; ++guard) x = parent[x];
+        label[i] = x;
+    }
+    return NE_OK;
+}
+
+int ne_world_stream(const NeWorld* w, void** stream) {
+    if (!w || !stream) return set_err(NE_ERR_ARG, "NULL argument");
+    *stream = (void*)w->stream;
+    return NE_OK;
+}
+
+int ne_world_launch_count(const NeWorld* w, uint64_t* launches) {
+    if (!w || !launches) return set_err(NE_ERR_ARG, "NULL argument");
+    *launches = w->launches;
+    return NE_OK;
+}
+
+}  // extern "C"

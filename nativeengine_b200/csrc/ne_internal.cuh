@@ -1,0 +1,104 @@
+// ne_internal.cuh -- device-side world layout and the host orchestration API
+// shared by the CUDA translation units of libne_cuda.so.
+//
+// HBM layout (one world):
+//   bodies   : structure of 32-byte records, one array per record kind, so a
+//              per-body kernel streams each array fully coalesced and a pair
+//              kernel gathers one 32-byte sector per record:
+//                pos  = (x, y, z, invMass)      quat = (w, x, y, z)
+//                vel  = (vx, vy, vz, -)         omg  = (wx, wy, wz, -)
+//                frc  = force accumulator       trq  = torque accumulator
+//                inert= (invIx, invIy, invIz, boundingRadius)
+//                geom = (radius, halfHeight, gravityScale, -)
+//                ext  = (halfExtents | plane normal, -)
+//                mat  = (friction, restitution, linearDamping, angularDamping)
+//                meta = (shape, flags, layer, mask)
+//   pairs    : CSR by first body -- pair_i/pair_j in sorted (i, j) order.
+//   contacts : 4 slots per surviving pair (normal+depth, point).
+//   constraints, warm cache, island order: flat arrays in solver order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ne_geom.cuh"
+#include "ne_cuda.h"
+
+namespace neb {
+
+// Internal body flag: the solver can change this body's velocity
+// (invMass > 0 or a nonzero inverse inertia).  Immovable bodies separate islands.
+constexpr uint32_t kFlagMutable = 1u << 16;
+
+// Device control block: capacity checks, counters, warm-cache selector.
+struct Ctl {
+    uint32_t abort;          // a capacity or bit budget was exceeded this step
+    uint32_t flags;          // bit0: EPA/clip budget overrun
+    uint32_t need_bits;      // sort-key bits the cell keys needed
+    uint32_t wsel;           // warm cache buffer holding the previous step
+    uint64_t P, S, C;        // pairs, survivors, contacts (totals, even if over capacity)
+    uint64_t islands, max_island, epa_cap_hits;
+    uint32_t wcount[2];      // warm cache entries per buffer
+    long long cmin[3], cmax[3];   // cell coordinate extents (open/reflective grid)
+    uint64_t scan_total;     // scratch total of the last scan
+};
+
+struct DevWorld {
+    // bodies
+    D4 *pos, *quat, *vel, *omg, *frc, *trq;
+    D4 *inert, *geom, *ext, *mat;
+    uint4* meta;
+    uint2* vrng;
+    D4* verts;
+    uint2* ncrng;
+    uint32_t* nc;
+    uint32_t* planes;        // indices of grid-excluded bodies, ascending
+    // pre-step snapshot (restored when a step is re-run)
+    D4 *s_pos, *s_quat, *s_vel, *s_omg, *s_frc, *s_trq;
+    // broadphase
+    unsigned long long *key[2];
+    uint32_t* val[2];
+    uint32_t *bcnt, *boff;
+    uint32_t *pair_i, *pair_j;
+    // narrowphase
+    uint32_t *pflag, *poff, *surv;
+    uint32_t *ccnt, *coff;
+    D4 *cn, *cp;             // 4 slots per survivor: (normal, depth), (point, -)
+    // constraints
+    uint32_t *ci, *cj, *cslot;
+    D4 *con_n;               // n, overlap
+    D4 *con_ra;              // rA, restBias
+    D4 *con_rb;              // rB, mu
+    D4 *con_p;               // contact point
+    double2* con_imp;        // nImp, tImp
+    // warm cache (double buffered)
+    unsigned long long* wkey[2];
+    double* wimp[2];
+    // islands
+    uint32_t* parent;
+    uint32_t *ilab[2], *iord[2];
+    uint32_t *iflag, *ioff, *istart;
+    // scratch
+    uint32_t *hist, *tsum;
+    Ctl* ctl;
+};
+
+struct Caps {
+    uint64_t P, S, C;
+};
+
+// Scan / sort primitives (ne_prims.cu).  All are asynchronous on `st`, all skip
+// when ctl->abort is set, and all count their launches into *launches.
+// Exclusive scan of n u32 values; the u64 total lands in *total (device).
+void scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tsum, uint64_t* total,
+              const Ctl* ctl, cudaStream_t st, uint64_t* launches);
+size_t scan_tsum_words(uint32_t n);
+// Stable LSD radix sort of (key, val) pairs on the low `bits` bits.
+// Ping-pongs between buffers 0 and 1; returns the buffer index holding the result.
+int radix_sort_u64(unsigned long long* key[2], uint32_t* val[2], uint32_t n, int bits, uint32_t* hist,
+                   uint32_t* tsum, const Ctl* ctl, cudaStream_t st, uint64_t* launches);
+int radix_sort_u32(uint32_t* key[2], uint32_t* val[2], uint32_t n, int bits, uint32_t* hist,
+                   uint32_t* tsum, const Ctl* ctl, cudaStream_t st, uint64_t* launches);
+size_t radix_hist_words(uint32_t n);
+
+}  // namespace neb

@@ -1,0 +1,820 @@
+// ne_step.cu -- the device kernels of one World::step() (src/world.cpp:133-146).
+//
+// Stage map (reference -> kernel):
+//   integrate()            src/world.cpp:373-411   k_integrate
+//   broadphasePairs()      src/world.cpp:424-501   k_cell_keys, radix sort, k_pair_count, k_pair_emit
+//   pair filters + cull    src/world.cpp:513-516   k_pair_cull, k_compact
+//   gatherContacts()       src/world.cpp:88-130    k_narrowphase (ne_geom.cuh)
+//   constraint build       src/world.cpp:537-553   k_constraint_build (+ union-find hooking)
+//   islands                src/world.cpp:332-343   k_island_label, radix sort, k_island_mark/_start
+//   warm start + 8 SI + position correction + warm-cache store
+//                          src/world.cpp:559-626   k_island_solve
+//   wrapPositions/applyWalls src/world.cpp:635-702 k_boundary
+//
+// Every kernel is a no-op once ctl->abort is set (a capacity overflow this
+// step); the host then restores the pre-step snapshot, grows the buffer and
+// re-runs the step, so an overflow never changes the result.
+#include "ne_step.cuh"
+
+namespace neb {
+
+namespace {
+
+constexpr int kT = 256;
+
+__device__ __forceinline__ V3 v3of(const D4& a) { return mk(a.x, a.y, a.z); }
+__device__ __forceinline__ Q qof(const D4& a) { return mkq(a.x, a.y, a.z, a.w); }
+__device__ __forceinline__ D4 d4of(const V3& v, double w) { D4 r; r.x = v.x; r.y = v.y; r.z = v.z; r.w = w; return r; }
+__device__ __forceinline__ D4 d4ofq(const Q& q) { D4 r; r.x = q.w; r.y = q.x; r.z = q.y; r.w = q.z; return r; }
+
+__device__ __forceinline__ bool grid_excluded(int shape) { return shape == SH_PLANE || shape == SH_MESH; }
+
+__device__ __forceinline__ BodyG load_geom(const DevWorld& d, uint32_t i) {
+    const D4 p = d.pos[i], q = d.quat[i], g = d.geom[i], e = d.ext[i];
+    const uint4 m = d.meta[i];
+    const uint2 vr = d.vrng[i];
+    BodyG b;
+    b.x = v3of(p);
+    b.q = qof(q);
+    b.he = v3of(e);
+    b.radius = g.x;
+    b.half_height = g.y;
+    b.verts = d.verts + vr.x;
+    b.nverts = (int)vr.y;
+    b.shape = (int)m.x;
+    return b;
+}
+
+__device__ __forceinline__ int bitlen_u64(unsigned long long x) { return x ? 64 - __clzll((long long)x) : 0; }
+
+// Per-axis cell coordinate (src/world.cpp:458-466).
+__device__ __forceinline__ long long cell_of(const StepArgs& a, double c, int axis) {
+    if (a.dom.periodic) {
+        long long k = (long long)floor((c + a.dom.half) / a.cell);
+        long long m = a.nc[axis];
+        return ((k % m) + m) % m;
+    }
+    return (long long)floor(c / a.cell);
+}
+
+// Compact sort key layout: a bijection of the reference's 21-bit-masked cell
+// coordinates (src/world.cpp:467-470) onto as few bits as the occupied range
+// needs, so the radix sort touches only varying digits.
+struct KeyLayout {
+    int bits[3];
+    long long base[3];
+    int total;
+};
+
+__device__ __forceinline__ KeyLayout key_layout(const StepArgs& a, const Ctl* ctl) {
+    KeyLayout L;
+    for (int ax = 0; ax < 3; ++ax) {
+        if (a.dom.periodic) {
+            const long long m = a.nc[ax];
+            L.bits[ax] = (m > (1ll << 21)) ? 21 : bitlen_u64((unsigned long long)(m - 1));
+            L.base[ax] = 0;
+        } else {
+            const long long span = ctl->cmax[ax] - ctl->cmin[ax];
+            L.bits[ax] = (span >= (1ll << 21) || span < 0) ? 21 : bitlen_u64((unsigned long long)span);
+            L.base[ax] = ctl->cmin[ax];
+        }
+    }
+    L.total = L.bits[0] + L.bits[1] + L.bits[2];
+    return L;
+}
+
+__device__ __forceinline__ unsigned long long compact_key(const KeyLayout& L, long long cx, long long cy,
+                                                          long long cz) {
+    const unsigned long long M = 0x1FFFFFull;
+    unsigned long long x = (unsigned long long)(cx - L.base[0]) & M;
+    unsigned long long y = (unsigned long long)(cy - L.base[1]) & M;
+    unsigned long long z = (unsigned long long)(cz - L.base[2]) & M;
+    return x | (y << L.bits[0]) | (z << (L.bits[0] + L.bits[1]));
+}
+
+__device__ __forceinline__ long long wrap_cell(const StepArgs& a, long long c, int axis) {
+    if (!a.dom.periodic) return c;
+    const long long m = a.nc[axis];
+    return ((c % m) + m) % m;
+}
+
+// The distinct neighbour keys of a cell (27 offsets; wrapping can alias them).
+__device__ __forceinline__ int neighbour_keys(const StepArgs& a, const KeyLayout& L, long long cx, long long cy,
+                                              long long cz, unsigned long long* out) {
+    int nk = 0;
+    for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dz = -1; dz <= 1; ++dz) {
+                unsigned long long k = compact_key(L, wrap_cell(a, cx + dx, 0), wrap_cell(a, cy + dy, 1),
+                                                   wrap_cell(a, cz + dz, 2));
+                bool dup = false;
+                for (int t = 0; t < nk; ++t) dup |= (out[t] == k);
+                if (!dup) out[nk++] = k;
+            }
+    return nk;
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u64(const unsigned long long* a, uint32_t lo, uint32_t hi,
+                                                    unsigned long long k) {
+    while (lo < hi) {
+        uint32_t mid = lo + ((hi - lo) >> 1);
+        if (a[mid] < k) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ uint32_t upper_bound_u64(const unsigned long long* a, uint32_t lo, uint32_t hi,
+                                                    unsigned long long k) {
+    while (lo < hi) {
+        uint32_t mid = lo + ((hi - lo) >> 1);
+        if (a[mid] <= k) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t lo, uint32_t hi, uint32_t k) {
+    while (lo < hi) {
+        uint32_t mid = lo + ((hi - lo) >> 1);
+        if (a[mid] < k) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t* a, uint32_t lo, uint32_t hi, uint32_t k) {
+    while (lo < hi) {
+        uint32_t mid = lo + ((hi - lo) >> 1);
+        if (a[mid] <= k) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+
+__global__ void k_step_begin(Ctl* ctl) {
+    ctl->abort = 0;
+    ctl->flags = 0;
+    ctl->need_bits = 0;
+    ctl->P = ctl->S = ctl->C = 0;
+    ctl->islands = 0;
+    ctl->max_island = 0;
+    ctl->epa_cap_hits = 0;
+    for (int a = 0; a < 3; ++a) {
+        ctl->cmin[a] = 0x7fffffffffffffffll;
+        ctl->cmax[a] = (long long)0x8000000000000000ull;
+    }
+}
+
+__device__ __forceinline__ long long warp_min_ll(long long v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        long long t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = t < v ? t : v;
+    }
+    return v;
+}
+__device__ __forceinline__ long long warp_max_ll(long long v) {
+    for (int o = 16; o > 0; o >>= 1) {
+        long long t = __shfl_xor_sync(0xffffffffu, v, o);
+        v = t > v ? t : v;
+    }
+    return v;
+}
+
+// World::integrate() (src/world.cpp:373-411) + pre-step snapshot + union-find
+// reset + cell extents of the post-integration positions.
+__global__ void __launch_bounds__(kT) k_integrate(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < a.n;
+    long long lo[3] = {0x7fffffffffffffffll, 0x7fffffffffffffffll, 0x7fffffffffffffffll};
+    long long hi[3] = {(long long)0x8000000000000000ull, (long long)0x8000000000000000ull,
+                       (long long)0x8000000000000000ull};
+    if (live) {
+        const DevWorld& d = a.d;
+        D4 p = d.pos[i], q4 = d.quat[i], v4 = d.vel[i], w4 = d.omg[i], f4 = d.frc[i], t4 = d.trq[i];
+        d.s_pos[i] = p; d.s_quat[i] = q4; d.s_vel[i] = v4; d.s_omg[i] = w4; d.s_frc[i] = f4; d.s_trq[i] = t4;
+        d.parent[i] = i;
+        const uint4 m = d.meta[i];
+        V3 x = v3of(p), v = v3of(v4), w = v3of(w4), F = v3of(f4), T = v3of(t4);
+        Q q = qof(q4);
+        const double invM = p.w, dt = a.dt;
+        if (m.y & NE_BODY_KINEMATIC) {
+            x = x + v * dt;
+            q = integrate_orientation(q, w, dt);
+        } else if (invM <= 0.0) {
+        } else {
+            const D4 I = d.inert[i], g = d.geom[i], mt = d.mat[i];
+            const V3 invI = v3of(I);
+            v = v + (a.g * g.z + F * invM) * dt;
+            x = x + v * dt;
+            V3 L = angular_momentum(q, invI, w);
+            L = L + T * dt;
+            q = integrate_orientation(q, w, dt);
+            w = apply_inv_inertia(q, invI, L);
+            if (mt.z > 0.0) v = v * (1.0 / (1.0 + mt.z * dt));
+            if (mt.w > 0.0) w = w * (1.0 / (1.0 + mt.w * dt));
+        }
+        F = mk(0.0, 0.0, 0.0);
+        T = F;
+        d.pos[i] = d4of(x, invM);
+        d.quat[i] = d4ofq(q);
+        d.vel[i] = d4of(v, 0.0);
+        d.omg[i] = d4of(w, 0.0);
+        d.frc[i] = d4of(F, 0.0);
+        d.trq[i] = d4of(T, 0.0);
+        if (!a.brute && !a.dom.periodic && !grid_excluded((int)m.x)) {
+            const double c[3] = {x.x, x.y, x.z};
+            for (int ax = 0; ax < 3; ++ax) lo[ax] = hi[ax] = cell_of(a, c[ax], ax);
+        }
+    }
+    if (!a.brute && !a.dom.periodic) {
+        for (int ax = 0; ax < 3; ++ax) {
+            long long mn = warp_min_ll(lo[ax]), mx = warp_max_ll(hi[ax]);
+            if ((threadIdx.x & 31) == 0 && mn <= mx) {
+                atomicMin(&ctl->cmin[ax], mn);
+                atomicMax(&ctl->cmax[ax], mx);
+            }
+        }
+    }
+}
+
+// Sort keys of the grid cells; grid-excluded bodies get a sentinel that sorts
+// after every real key.
+__global__ void __launch_bounds__(kT) k_cell_keys(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const KeyLayout L = key_layout(a, ctl);
+    if (i == 0) {
+        ctl->need_bits = (uint32_t)(L.total + 1);
+        if (L.total + 1 > a.key_bits) ctl->abort = 1;
+    }
+    if (i >= a.n) return;
+    const D4 p = a.d.pos[i];
+    const int shape = (int)a.d.meta[i].x;
+    unsigned long long k;
+    if (grid_excluded(shape)) {
+        k = 1ull << L.total;
+    } else {
+        k = compact_key(L, cell_of(a, p.x, 0), cell_of(a, p.y, 1), cell_of(a, p.z, 2));
+    }
+    a.d.key[0][i] = k;
+    a.d.val[0][i] = i;
+}
+
+// Number of partners j > i of body i (the sorted unique pair list is the CSR
+// of these partner lists).
+__global__ void __launch_bounds__(kT) k_pair_count(StepArgs a, int kb) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const DevWorld& d = a.d;
+    if (a.brute || grid_excluded((int)d.meta[i].x)) {
+        d.bcnt[i] = a.n - 1 - i;
+        return;
+    }
+    const KeyLayout L = key_layout(a, ctl);
+    const D4 p = d.pos[i];
+    unsigned long long nk[27];
+    const int m = neighbour_keys(a, L, cell_of(a, p.x, 0), cell_of(a, p.y, 1), cell_of(a, p.z, 2), nk);
+    const unsigned long long* keys = d.key[kb];
+    const uint32_t* vals = d.val[kb];
+    uint32_t cnt = 0;
+    for (int t = 0; t < m; ++t) {
+        uint32_t lo = lower_bound_u64(keys, 0, a.n, nk[t]);
+        uint32_t hi = upper_bound_u64(keys, lo, a.n, nk[t]);
+        if (lo == hi) continue;
+        uint32_t s = upper_bound_u32(vals, lo, hi, i);
+        cnt += hi - s;
+    }
+    cnt += a.nplanes - upper_bound_u32(d.planes, 0, a.nplanes, i);
+    d.bcnt[i] = cnt;
+}
+
+// Writes body i's sorted partner list at its CSR offset.  One warp per body:
+// lanes 0..26 own one neighbour cell run each, lane 27 the plane list; every
+// partner's output rank is the number of smaller partners over all runs.
+__global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    if (ctl->P > a.Pcap) {
+        if (threadIdx.x == 0 && blockIdx.x == 0) ctl->abort = 1;
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= a.n) return;
+    const DevWorld& d = a.d;
+    const uint32_t base = d.boff[i];
+    if (a.brute || grid_excluded((int)d.meta[i].x)) {
+        const uint32_t cnt = a.n - 1 - i;
+        for (uint32_t k = lane; k < cnt; k += 32) {
+            d.pair_i[base + k] = i;
+            d.pair_j[base + k] = i + 1 + k;
+        }
+        return;
+    }
+    const KeyLayout L = key_layout(a, ctl);
+    const D4 p = d.pos[i];
+    const long long cx = cell_of(a, p.x, 0), cy = cell_of(a, p.y, 1), cz = cell_of(a, p.z, 2);
+    const unsigned long long* keys = d.key[kb];
+    const uint32_t* vals = d.val[kb];
+    // Lane t < 27 takes neighbour offset t; duplicates (wrap aliasing) keep
+    // only their lowest lane.
+    uint32_t rlo = 0, rhi = 0;
+    const uint32_t* src = vals;
+    if (lane < 27) {
+        const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+        unsigned long long k = compact_key(L, wrap_cell(a, cx + dx, 0), wrap_cell(a, cy + dy, 1),
+                                           wrap_cell(a, cz + dz, 2));
+        const uint32_t grp = __match_any_sync(0x07ffffffu, k);
+        if (lane == __ffs(grp) - 1) {
+            uint32_t lo = lower_bound_u64(keys, 0, a.n, k);
+            uint32_t hi = upper_bound_u64(keys, lo, a.n, k);
+            rlo = (lo < hi) ? upper_bound_u32(vals, lo, hi, i) : hi;
+            rhi = hi;
+        }
+    } else if (lane == 27) {
+        src = d.planes;
+        rlo = upper_bound_u32(d.planes, 0, a.nplanes, i);
+        rhi = a.nplanes;
+    }
+    const uint32_t len = rhi - rlo;
+    // Each lane walks the elements of its own run; the rank of element x is
+    // its index in its run plus the count of smaller elements in other runs.
+    for (uint32_t e = 0;; ++e) {   // ends after the longest run (at most n - 1 rounds)
+        // Round e: every lane takes the e-th element of its run, if any.
+        const bool has = e < len;
+        if (!__any_sync(0xffffffffu, has)) break;
+        uint32_t x = has ? src[rlo + e] : 0u;
+        uint32_t rank = e;
+        // Count elements < x in the other lanes' runs.
+        for (int r = 0; r < 28; ++r) {
+            const uint32_t olo = __shfl_sync(0xffffffffu, rlo, r);
+            const uint32_t ohi = __shfl_sync(0xffffffffu, rhi, r);
+            if (r == lane || !has || olo == ohi) continue;
+            const uint32_t* os = (r == 27) ? d.planes : vals;
+            rank += lower_bound_u32(os, olo, ohi, x) - olo;
+        }
+        if (has) {
+            d.pair_i[base + rank] = i;
+            d.pair_j[base + rank] = x;
+        }
+    }
+}
+
+// Pair filters (src/world.cpp:513-516) and a conservative bounding-volume cull
+// that only removes pairs the narrowphase provably reports as separated.
+__global__ void __launch_bounds__(kT) k_pair_cull(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t pidx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pidx >= a.Pcap) return;
+    const DevWorld& d = a.d;
+    uint32_t keep = 0;
+    if (pidx < ctl->P) {
+        const uint32_t i = d.pair_i[pidx], j = d.pair_j[pidx];
+        const D4 pa = d.pos[i], pb = d.pos[j];
+        const uint4 ma = d.meta[i], mb = d.meta[j];
+        keep = 1;
+        if (pa.w + pb.w <= 0.0) keep = 0;
+        if (!((ma.w & (1u << (mb.z & 31u))) && (mb.w & (1u << (ma.z & 31u))))) keep = 0;
+        if (keep) {
+            const uint2 nr = d.ncrng[i];
+            for (uint32_t k = 0; k < nr.y; ++k)
+                if (d.nc[nr.x + k] == j) { keep = 0; break; }
+        }
+        if ((ma.y | mb.y) & NE_BODY_SENSOR) keep = 0;
+        const int sa = (int)ma.x, sb = (int)mb.x;
+        if (keep && sa == SH_PLANE && sb == SH_PLANE) keep = 0;
+        if (keep && sa != SH_PLANE && sb != SH_PLANE) {
+            // Bounding spheres about the centres (nearest image).
+            const double ra = d.inert[i].w, rb = d.inert[j].w;
+            const V3 dd = min_image(a.dom, mk(pb.x - pa.x, pb.y - pa.y, pb.z - pa.z));
+            const double r = (ra + rb) * (1.0 + 1e-9) + 1e-9;
+            if (norm2(dd) > r * r) keep = 0;
+            // Box vs bounding sphere: distance from the sphere centre to the box.
+            if (keep && (sa == SH_BOX || sb == SH_BOX)) {
+                const bool boxA = (sa == SH_BOX);
+                const uint32_t bi = boxA ? i : j;
+                const double rs = boxA ? rb : ra;
+                const V3 rel = boxA ? dd : -dd;     // other centre relative to the box centre
+                const Q qb = qof(d.quat[bi]);
+                const V3 he = v3of(d.ext[bi]);
+                const V3 l = inv_rotate(qb, rel);
+                const double ex = fmax(fabs(l.x) - he.x, 0.0), ey = fmax(fabs(l.y) - he.y, 0.0),
+                             ez = fmax(fabs(l.z) - he.z, 0.0);
+                const double lim = rs * (1.0 + 1e-9) + 1e-9 * (1.0 + norm(he));
+                if (ex * ex + ey * ey + ez * ez > lim * lim) keep = 0;
+            }
+        }
+    }
+    d.pflag[pidx] = keep;
+}
+
+__global__ void __launch_bounds__(kT) k_compact(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t pidx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ctl->S > a.Scap) {
+        if (pidx == 0) ctl->abort = 1;
+        return;
+    }
+    if (pidx >= a.Pcap) return;
+    if (a.d.pflag[pidx]) a.d.surv[a.d.poff[pidx]] = (uint32_t)pidx;
+}
+
+// gatherContacts() for one surviving pair (src/world.cpp:122-129).
+__global__ void __launch_bounds__(128) k_narrowphase(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.Scap) return;
+    const DevWorld& d = a.d;
+    if (s >= ctl->S) {
+        d.ccnt[s] = 0;
+        return;
+    }
+    const uint32_t pidx = d.surv[s];
+    const uint32_t i = d.pair_i[pidx], j = d.pair_j[pidx];
+    const BodyG A = load_geom(d, i), B = load_geom(d, j);
+    EpaScratch S;
+    int fl = 0;
+    Contact c = detect_contact(A, B, a.dom, S, fl);
+    uint32_t cnt = 0;
+    if (c.hit) {
+        if (A.shape == SH_BOX && B.shape == SH_BOX) {
+            Manifold m = box_box_manifold(A, B, c.normal, a.dom, fl);
+            for (int k = 0; k < m.count; ++k) {
+                d.cn[4 * s + k] = d4of(c.normal, m.depth[k]);
+                d.cp[4 * s + k] = d4of(m.point[k], 0.0);
+            }
+            cnt = (uint32_t)m.count;
+        }
+        if (cnt == 0) {
+            d.cn[4 * s] = d4of(c.normal, c.overlap);
+            d.cp[4 * s] = d4of(c.point, 0.0);
+            cnt = 1;
+        }
+    }
+    d.ccnt[s] = cnt;
+    if (fl & 1) atomicOr(&ctl->flags, 1u);
+    if (fl & 2) atomicAdd((unsigned long long*)&ctl->epa_cap_hits, 1ull);
+}
+
+__device__ __forceinline__ double combine_mat(int mode, double x, double y) {
+    switch (mode) {
+        case NE_COMBINE_AVERAGE: return 0.5 * (x + y);
+        case NE_COMBINE_MIN: return x < y ? x : y;
+        case NE_COMBINE_MAX: return x > y ? x : y;
+        case NE_COMBINE_MULTIPLY: return x * y;
+        case NE_COMBINE_GEOMETRIC_MEAN: return sqrt((x > 0 ? x : 0) * (y > 0 ? y : 0));
+    }
+    return 0.5 * (x + y);
+}
+
+__device__ __forceinline__ uint32_t uf_find(uint32_t* parent, uint32_t x) {
+    volatile uint32_t* p = parent;
+    while (true) {
+        uint32_t px = p[x];
+        if (px == x) return x;
+        uint32_t gp = p[px];
+        if (gp != px) p[x] = gp;   // path halving; gp is an ancestor, so the race is benign
+        x = px;
+    }
+}
+
+// Link the components of a and b; the root is always the smaller index, so
+// every component's root is its minimum body index.
+__device__ __forceinline__ void uf_union(uint32_t* parent, uint32_t a, uint32_t b) {
+    while (true) {
+        a = uf_find(parent, a);
+        b = uf_find(parent, b);
+        if (a == b) return;
+        if (a > b) { uint32_t t = a; a = b; b = t; }
+        uint32_t old = atomicCAS(&parent[b], b, a);
+        if (old == b) return;
+        b = old;
+    }
+}
+
+// Contact constraints of one surviving pair (src/world.cpp:518-553): lever
+// arms, restitution bias from the pre-solve velocities, combined material,
+// warm-start impulse looked up in the previous step's sorted cache.
+__global__ void __launch_bounds__(kT) k_constraint_build(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ctl->C > a.Ccap) {
+        if (s == 0) ctl->abort = 1;
+        return;
+    }
+    if (s >= ctl->S) return;
+    const DevWorld& d = a.d;
+    const uint32_t cnt = d.ccnt[s];
+    if (cnt == 0) return;
+    const uint32_t pidx = d.surv[s];
+    const uint32_t i = d.pair_i[pidx], j = d.pair_j[pidx];
+    const D4 pa = d.pos[i], pb = d.pos[j];
+    const V3 xa = v3of(pa), xb = v3of(pb);
+    const V3 va = v3of(d.vel[i]), vb = v3of(d.vel[j]), wa = v3of(d.omg[i]), wb = v3of(d.omg[j]);
+    const D4 ma = d.mat[i], mb = d.mat[j];
+    const double ea = ma.y < 0 ? a.restitution : ma.y, eb = mb.y < 0 ? a.restitution : mb.y;
+    const double fa = ma.x < 0 ? a.friction : ma.x, fb = mb.x < 0 ? a.friction : mb.x;
+    const double e = combine_mat(a.rcomb, ea, eb);
+    const double mu = combine_mat(a.fcomb, fa, fb);
+    const uint32_t fla = d.meta[i].y, flb = d.meta[j].y;
+    if ((fla & kFlagMutable) && (flb & kFlagMutable)) uf_union(d.parent, i, j);
+    const unsigned long long key = ((unsigned long long)i << 32) | (unsigned long long)j;
+    const uint32_t c0 = d.coff[s];
+    const uint32_t ws = ctl->wsel;
+    const uint32_t wn = ctl->wcount[ws];
+    uint32_t widx = 0;
+    if (a.warm) widx = lower_bound_u64(d.wkey[ws], 0, wn, key);
+    for (uint32_t k = 0; k < cnt; ++k) {
+        const uint32_t c = c0 + k;
+        const D4 cn = d.cn[4 * s + k];
+        const V3 n = v3of(cn), pt = v3of(d.cp[4 * s + k]);
+        const V3 rA = min_image(a.dom, pt - xa);
+        const V3 rB = min_image(a.dom, pt - xb);
+        const V3 vc = (va + cross(wa, rA)) - (vb + cross(wb, rB));
+        const double vn = dot(vc, n);
+        const double restBias = (vn < -0.5) ? -e * vn : 0.0;
+        double nImp = 0.0;
+        if (a.warm && widx + k < wn && d.wkey[ws][widx + k] == key) nImp = d.wimp[ws][widx + k];
+        d.ci[c] = i;
+        d.cj[c] = j;
+        d.cslot[c] = k;
+        d.con_n[c] = cn;
+        d.con_ra[c] = d4of(rA, restBias);
+        d.con_rb[c] = d4of(rB, mu);
+        d.con_p[c] = d4of(pt, 0.0);
+        d.con_imp[c] = make_double2(nImp, 0.0);
+        d.wkey[ws ^ 1][c] = key;
+    }
+}
+
+// Island label of every constraint (root of its first mutable body) and the
+// identity order; padding entries get label n so they sort last.
+__global__ void __launch_bounds__(kT) k_island_label(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= a.Ccap) return;
+    const DevWorld& d = a.d;
+    uint32_t lab = a.n;
+    if (c < ctl->C) {
+        const uint32_t i = d.ci[c], j = d.cj[c];
+        lab = (d.meta[i].y & kFlagMutable) ? uf_find(d.parent, i) : uf_find(d.parent, j);
+    }
+    d.ilab[0][c] = lab;
+    d.iord[0][c] = (uint32_t)c;
+}
+
+__global__ void __launch_bounds__(kT) k_island_mark(StepArgs a, int ib) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.Ccap) return;
+    const uint32_t* lab = a.d.ilab[ib];
+    uint32_t f = 0;
+    if (k < ctl->C) f = (k == 0 || lab[k] != lab[k - 1]) ? 1u : 0u;
+    a.d.iflag[k] = f;
+}
+
+__global__ void __launch_bounds__(kT) k_island_start(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t C = ctl->C;
+    if (k == 0) {
+        ctl->islands = ctl->scan_total;
+        a.d.istart[ctl->scan_total] = (uint32_t)C;
+    }
+    if (k < C && a.d.iflag[k]) a.d.istart[a.d.ioff[k]] = (uint32_t)k;
+}
+
+struct BodyS {
+    V3 v, w;
+    Q q;
+    V3 invI;
+    double invM;
+    bool mut;
+};
+
+__device__ __forceinline__ BodyS load_solver_body(const DevWorld& d, uint32_t i) {
+    BodyS b;
+    b.v = v3of(d.vel[i]);
+    b.w = v3of(d.omg[i]);
+    b.q = qof(d.quat[i]);
+    const D4 I = d.inert[i];
+    b.invI = v3of(I);
+    b.invM = d.pos[i].w;
+    b.mut = (d.meta[i].y & kFlagMutable) != 0;
+    return b;
+}
+
+// effMass (src/contact.hpp:28-33).
+__device__ __forceinline__ double eff_mass(const BodyS& A, const BodyS& B, const V3& ra, const V3& rb,
+                                           const V3& u) {
+    V3 angA = cross(apply_inv_inertia(A.q, A.invI, cross(ra, u)), ra);
+    V3 angB = cross(apply_inv_inertia(B.q, B.invI, cross(rb, u)), rb);
+    return A.invM + B.invM + dot(angA + angB, u);
+}
+
+__device__ __forceinline__ void apply_pair_impulse(BodyS& A, BodyS& B, const V3& ra, const V3& rb, const V3& J) {
+    A.v = A.v + J * A.invM;
+    A.w = A.w + apply_inv_inertia(A.q, A.invI, cross(ra, J));
+    B.v = B.v - J * B.invM;
+    B.w = B.w - apply_inv_inertia(B.q, B.invI, cross(rb, J));
+}
+
+__device__ __forceinline__ void store_solver_body(const DevWorld& d, uint32_t i, const BodyS& b) {
+    if (!b.mut) return;   // immovable: +-0 updates leave it unchanged; never written (shared by islands)
+    d.vel[i] = d4of(b.v, 0.0);
+    d.omg[i] = d4of(b.w, 0.0);
+}
+
+// One thread per island: warm start (src/world.cpp:559-568), 8 Gauss-Seidel
+// sweeps in the reference's constraint order (:572-612), position correction
+// (:615-616), and the impulses for the warm-cache store (:619-626).  Islands
+// share no mutable body, so running them concurrently reproduces the
+// reference's single global sweep exactly.
+__global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ctl->islands) return;
+    const DevWorld& d = a.d;
+    const uint32_t s = d.istart[t], e = d.istart[t + 1];
+    const uint32_t* ord = d.iord[ib];
+    atomicMax((unsigned long long*)&ctl->max_island, (unsigned long long)(e - s));
+
+    if (a.warm) {
+        for (uint32_t k = s; k < e; ++k) {
+            const uint32_t c = ord[k];
+            const double nImp = d.con_imp[c].x;
+            if (nImp == 0.0) continue;
+            const uint32_t i = d.ci[c], j = d.cj[c];
+            BodyS A = load_solver_body(d, i), B = load_solver_body(d, j);
+            const V3 n = v3of(d.con_n[c]), rA = v3of(d.con_ra[c]), rB = v3of(d.con_rb[c]);
+            apply_pair_impulse(A, B, rA, rB, n * nImp);
+            store_solver_body(d, i, A);
+            store_solver_body(d, j, B);
+        }
+    }
+    for (int it = 0; it < 8; ++it) {
+        for (uint32_t k = s; k < e; ++k) {
+            const uint32_t c = ord[k];
+            const uint32_t i = d.ci[c], j = d.cj[c];
+            BodyS A = load_solver_body(d, i), B = load_solver_body(d, j);
+            const D4 cn = d.con_n[c], ra4 = d.con_ra[c], rb4 = d.con_rb[c];
+            const V3 n = v3of(cn), rA = v3of(ra4), rB = v3of(rb4);
+            const double restBias = ra4.w, mu = rb4.w;
+            double2 imp = d.con_imp[c];
+            const V3 vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+            const double vn = dot(vc, n);
+            const double Kn = eff_mass(A, B, rA, rB, n);
+            if (Kn > 1e-18) {
+                double dj = (restBias - vn) / Kn;
+                const double old = imp.x;
+                imp.x = (old + dj > 0.0) ? old + dj : 0.0;
+                dj = imp.x - old;
+                apply_pair_impulse(A, B, rA, rB, n * dj);
+            }
+            if (mu > 0.0 && imp.x > 0.0) {
+                const V3 vc2 = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+                const V3 vt = vc2 - n * dot(vc2, n);
+                const double vtl = norm(vt);
+                if (vtl > 1e-12) {
+                    const V3 tg = vt / vtl;
+                    const double Kt = eff_mass(A, B, rA, rB, tg);
+                    if (Kt > 1e-18) {
+                        double djt = -vtl / Kt;
+                        const double maxF = mu * imp.x;
+                        const double old = imp.y;
+                        const double sum = old + djt;
+                        imp.y = (sum < -maxF) ? -maxF : (sum > maxF ? maxF : sum);
+                        djt = imp.y - old;
+                        apply_pair_impulse(A, B, rA, rB, tg * djt);
+                    }
+                }
+            }
+            d.con_imp[c] = imp;
+            store_solver_body(d, i, A);
+            store_solver_body(d, j, B);
+        }
+    }
+    // correctPenetration (src/contact.hpp:78-85), in constraint order.
+    for (uint32_t k = s; k < e; ++k) {
+        const uint32_t c = ord[k];
+        const uint32_t i = d.ci[c], j = d.cj[c];
+        const D4 pa = d.pos[i], pb = d.pos[j];
+        const double invSum = pa.w + pb.w;
+        const D4 cn = d.con_n[c];
+        const double overlap = cn.w;
+        if (!(invSum <= 0.0 || overlap <= 0.0)) {
+            const V3 corr = v3of(cn) * (a.beta * overlap / invSum);
+            if (d.meta[i].y & kFlagMutable) d.pos[i] = d4of(v3of(pa) + corr * pa.w, pa.w);
+            if (d.meta[j].y & kFlagMutable) d.pos[j] = d4of(v3of(pb) - corr * pb.w, pb.w);
+        }
+        if (a.warm) d.wimp[ctl->wsel ^ 1][c] = d.con_imp[c].x;
+    }
+}
+
+// wrapPositions() / applyWalls() (src/world.cpp:698-702, 635-657).
+__global__ void __launch_bounds__(kT) k_boundary(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const DevWorld& d = a.d;
+    D4 p = d.pos[i];
+    if (!(p.w > 0.0)) return;
+    if (a.dom.periodic) {
+        V3 x = wrap(a.dom, v3of(p));
+        d.pos[i] = d4of(x, p.w);
+        return;
+    }
+    if (a.open_boundary) return;
+    BodyG b = load_geom(d, i);
+    D4 v4 = d.vel[i];
+    double px[3] = {p.x, p.y, p.z};
+    double pv[3] = {v4.x, v4.y, v4.z};
+    const double h = a.dom.half;
+    for (int axis = 0; axis < 3; ++axis) {
+        for (int sgn = -1; sgn <= 1; sgn += 2) {
+            V3 outward = mk(axis == 0 ? double(sgn) : 0.0, axis == 1 ? double(sgn) : 0.0,
+                            axis == 2 ? double(sgn) : 0.0);
+            b.x = mk(px[0], px[1], px[2]);
+            V3 sp = support_world(b, outward);
+            double coord = (axis == 0 ? sp.x : axis == 1 ? sp.y : sp.z) * sgn;
+            double pen = coord - h;
+            if (pen > 0.0) {
+                px[axis] -= double(sgn) * pen;
+                if (pv[axis] * sgn > 0.0) pv[axis] = -a.restitution * pv[axis];
+            }
+        }
+    }
+    d.pos[i] = d4of(mk(px[0], px[1], px[2]), p.w);
+    d.vel[i] = d4of(mk(pv[0], pv[1], pv[2]), 0.0);
+}
+
+__global__ void k_step_end(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    if (a.warm) {
+        const uint32_t nw = ctl->wsel ^ 1;
+        ctl->wcount[nw] = (uint32_t)ctl->C;
+        ctl->wsel = nw;
+    }
+}
+
+inline uint32_t blocks_for(uint64_t n, int t) { return (uint32_t)((n + t - 1) / t); }
+
+}  // namespace
+
+// Enqueue one step.  The host reads ctl afterwards to learn whether it must
+// be re-run with larger buffers.
+void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches) {
+    StepArgs a = a0;
+    const DevWorld& d = a.d;
+    Ctl* ctl = d.ctl;
+    uint64_t& L = *launches;
+    k_step_begin<<<1, 1, 0, st>>>(ctl); ++L;
+    k_integrate<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
+
+    // Broadphase: cell keys -> stable sort -> per-body partner counts -> CSR.
+    int kb = 0;
+    if (!a.brute) {
+        k_cell_keys<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
+        unsigned long long* keys[2] = {d.key[0], d.key[1]};
+        uint32_t* vals[2] = {d.val[0], d.val[1]};
+        kb = radix_sort_u64(keys, vals, a.n, a.key_bits, d.hist, d.tsum, ctl, st, launches);
+    }
+    k_pair_count<<<blocks_for(a.n, kT), kT, 0, st>>>(a, kb); ++L;
+    scan_u32(d.bcnt, d.boff, a.n, d.tsum, &ctl->P, ctl, st, launches);
+    k_pair_emit<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a, kb); ++L;
+
+    // Narrowphase on the pairs that survive the filters and the cull.
+    k_pair_cull<<<blocks_for(a.Pcap, kT), kT, 0, st>>>(a); ++L;
+    scan_u32(d.pflag, d.poff, (uint32_t)a.Pcap, d.tsum, &ctl->S, ctl, st, launches);
+    k_compact<<<blocks_for(a.Pcap, kT), kT, 0, st>>>(a); ++L;
+    k_narrowphase<<<blocks_for(a.Scap, 128), 128, 0, st>>>(a); ++L;
+    scan_u32(d.ccnt, d.coff, (uint32_t)a.Scap, d.tsum, &ctl->C, ctl, st, launches);
+    k_constraint_build<<<blocks_for(a.Scap, kT), kT, 0, st>>>(a); ++L;
+
+    // Islands: label, stable sort by label, segment starts.
+    k_island_label<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a); ++L;
+    int lbits = 1;
+    while ((1ull << lbits) <= (unsigned long long)a.n) ++lbits;
+    uint32_t* labs[2] = {d.ilab[0], d.ilab[1]};
+    uint32_t* ords[2] = {d.iord[0], d.iord[1]};
+    const int ib = radix_sort_u32(labs, ords, (uint32_t)a.Ccap, lbits, d.hist, d.tsum, ctl, st, launches);
+    k_island_mark<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a, ib); ++L;
+    scan_u32(d.iflag, d.ioff, (uint32_t)a.Ccap, d.tsum, &ctl->scan_total, ctl, st, launches);
+    k_island_start<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a); ++L;
+    k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib); ++L;
+
+    k_boundary<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
+    k_step_end<<<1, 1, 0, st>>>(a); ++L;
+}
+
+}  // namespace neb

@@ -1,0 +1,133 @@
+"""Python handle on one device world, over the C-ABI of libne_cuda.so.
+
+This is test and benchmark plumbing around ``include/ne_cuda.h``; the C++17
+facade (``host/include/ne/world.hpp``) is the reference-compatible API.  Every
+call goes to the CUDA path -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import _ffi
+from .bodies import BodyArrays, default_params
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class DeviceWorld:
+    def __init__(self, params: Optional[_ffi.NeWorldParams] = None, bodies: Optional[BodyArrays] = None):
+        self._lib = _ffi.load()
+        self.params = params if params is not None else default_params()
+        h = C.c_void_p()
+        _ffi.check(self._lib.ne_world_create(C.byref(self.params), C.byref(h)), "ne_world_create")
+        self._h = h
+        self.n = 0
+        if bodies is not None:
+            self.upload(bodies)
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ne_world_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_params(self, params: _ffi.NeWorldParams):
+        self.params = params
+        _ffi.check(self._lib.ne_world_set_params(self._h, C.byref(params)), "ne_world_set_params")
+
+    def upload(self, bodies: BodyArrays):
+        self._bodies = bodies
+        self.n = bodies.n
+        _ffi.check(self._lib.ne_world_upload(self._h, C.byref(bodies.c)), "ne_world_upload")
+
+    def upload_state(self, x=None, q=None, v=None, w=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (x, q, v, w)]
+        _ffi.check(self._lib.ne_world_upload_state(self._h, *[_ptr(a) for a in arrs]), "ne_world_upload_state")
+
+    # -- stepping ------------------------------------------------------------
+    def step(self, nsteps: int = 1) -> int:
+        rc = self._lib.ne_world_step(self._h, int(nsteps))
+        if rc not in (_ffi.NE_OK, _ffi.NE_ERR_NUMERIC):
+            _ffi.check(rc, "ne_world_step")
+        return rc
+
+    def reset_warm_cache(self):
+        _ffi.check(self._lib.ne_world_reset_warm_cache(self._h), "ne_world_reset_warm_cache")
+
+    # -- readback ------------------------------------------------------------
+    def state(self, with_forces: bool = False) -> Dict[str, np.ndarray]:
+        n = self.n
+        out = {"x": np.empty((n, 3)), "q": np.empty((n, 4)), "v": np.empty((n, 3)), "w": np.empty((n, 3))}
+        if with_forces:
+            out["force"] = np.empty((n, 3))
+            out["torque"] = np.empty((n, 3))
+        s = _ffi.NeBodyArrays()
+        s.n = n
+        for k, a in out.items():
+            setattr(s, k, a.ctypes.data_as(C.POINTER(C.c_double)))
+        _ffi.check(self._lib.ne_world_download(self._h, C.byref(s)), "ne_world_download")
+        return out
+
+    def stats(self) -> Dict[str, int]:
+        st = _ffi.NeStepStats()
+        _ffi.check(self._lib.ne_world_stats(self._h, C.byref(st)), "ne_world_stats")
+        return {name: int(getattr(st, name)) for name, _ in st._fields_}
+
+    def pairs(self) -> np.ndarray:
+        cnt = C.c_uint64()
+        _ffi.check(self._lib.ne_world_pairs(self._h, None, None, 0, C.byref(cnt)), "ne_world_pairs")
+        P = cnt.value
+        pi = np.empty(P, dtype=np.uint32)
+        pj = np.empty(P, dtype=np.uint32)
+        _ffi.check(self._lib.ne_world_pairs(self._h, _ptr(pi), _ptr(pj), P, C.byref(cnt)), "ne_world_pairs")
+        return np.stack([pi, pj], axis=1)
+
+    def contacts(self) -> Dict[str, np.ndarray]:
+        cnt = C.c_uint64()
+        empty = _ffi.NeContactArrays()
+        _ffi.check(self._lib.ne_world_contacts(self._h, C.byref(empty), 0, C.byref(cnt)), "ne_world_contacts")
+        m = cnt.value
+        out = {
+            "i": np.empty(m, np.uint32), "j": np.empty(m, np.uint32), "slot": np.empty(m, np.uint32),
+            "point": np.empty((m, 3)), "normal": np.empty((m, 3)), "depth": np.empty(m),
+            "n_imp": np.empty(m), "t_imp": np.empty(m),
+        }
+        s = _ffi.NeContactArrays()
+        for k in ("i", "j", "slot"):
+            setattr(s, k, out[k].ctypes.data_as(C.POINTER(C.c_uint32)))
+        for k in ("point", "normal", "depth", "n_imp", "t_imp"):
+            setattr(s, k, out[k].ctypes.data_as(C.POINTER(C.c_double)))
+        _ffi.check(self._lib.ne_world_contacts(self._h, C.byref(s), m, C.byref(cnt)), "ne_world_contacts")
+        return out
+
+    def islands(self) -> np.ndarray:
+        lab = np.empty(self.n, dtype=np.uint32)
+        _ffi.check(self._lib.ne_world_islands(self._h, _ptr(lab), self.n), "ne_world_islands")
+        return lab
+
+    def stream_handle(self) -> int:
+        s = C.c_void_p()
+        _ffi.check(self._lib.ne_world_stream(self._h, C.byref(s)), "ne_world_stream")
+        return s.value or 0
+
+    def launch_count(self) -> int:
+        v = C.c_uint64()
+        _ffi.check(self._lib.ne_world_launch_count(self._h, C.byref(v)), "ne_world_launch_count")
+        return int(v.value)
