@@ -215,6 +215,17 @@ int ne_world_stream(const NeWorld* world, void** stream);
 /* Number of kernel launches made by the last ne_world_step call. */
 int ne_world_launch_count(const NeWorld* world, uint64_t* launches);
 
+/* Per-stage device timing (CUDA events on the world's stream).  Stages:
+ * 0 integrate, 1 broadphase, 2 pair filter + cull, 3 narrowphase,
+ * 4 constraint build, 5 islands, 6 solve, 7 boundary.  While enabled, each
+ * step records NE_NUM_STAGES + 1 events; ne_world_stage_times returns the
+ * accumulated milliseconds per stage and the number of steps timed since the
+ * last enable.  No counterpart in the reference (it has no timers). */
+#define NE_NUM_STAGES 8
+int ne_world_profile(NeWorld* world, int enable);
+int ne_world_stage_times(NeWorld* world, double* ms, uint64_t* steps);
+const char* ne_stage_name(int stage);
+
 /* Human-readable status / last CUDA error text. */
 const char* ne_status_string(int status);
 const char* ne_last_error(void);

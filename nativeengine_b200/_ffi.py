@@ -22,6 +22,7 @@ NE_ERR_UNSUPPORTED = 4
 NE_ERR_TIMEOUT = 5
 NE_ERR_NUMERIC = 6
 NE_ERR_NO_DEVICE = 7
+NUM_STAGES = 8
 
 # shapes (ne::Shape order)
 SPHERE, CYLINDER, BOX, CAPSULE, CONVEX, PLANE, MESH, COMPOUND = range(8)
@@ -107,6 +108,9 @@ EXPORTS = {
     "ne_world_islands": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "ne_world_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "ne_world_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "ne_world_profile": (C.c_int, [C.c_void_p, C.c_int]),
+    "ne_world_stage_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    "ne_stage_name": (C.c_char_p, [C.c_int]),
     "ne_status_string": (C.c_char_p, [C.c_int]),
     "ne_last_error": (C.c_char_p, []),
 }

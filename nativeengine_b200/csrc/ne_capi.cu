@@ -73,6 +73,11 @@ struct NeWorld {
     NeStepStats stats{};
     uint64_t launches = 0;
     bool has_bodies = false;
+    // stage timing
+    bool profile = false;
+    cudaEvent_t ev[NE_NUM_STAGES + 1] = {};
+    double stage_ms[NE_NUM_STAGES] = {};
+    uint64_t stage_steps = 0;
 };
 
 namespace {
@@ -319,6 +324,8 @@ int ne_world_destroy(NeWorld* w) {
     for (int b = 0; b < 2; ++b) { dfree(d.wkey[b]); dfree(d.wimp[b]); }
     dfree(d.hist); dfree(d.tsum); dfree(d.ctl);
     if (w->h_ctl) cudaFreeHost(w->h_ctl);
+    for (int k = 0; k <= NE_NUM_STAGES; ++k)
+        if (w->ev[k]) cudaEventDestroy(w->ev[k]);
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
     return NE_OK;
@@ -556,7 +563,7 @@ int ne_world_step(NeWorld* w, uint32_t nsteps) {
         for (int attempt = 0;; ++attempt) {
             if (attempt > 16) return set_err(NE_ERR_CAPACITY, "step did not fit after repeated growth");
             neb::StepArgs a = make_args(w);
-            neb::launch_step(a, w->stream, &w->launches);
+            neb::launch_step(a, w->stream, &w->launches, w->profile ? w->ev : nullptr);
             NE_CUDA_TRY(cudaGetLastError());
             NE_CUDA_TRY(cudaMemcpyAsync(w->h_ctl, w->d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost, w->stream));
             NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
@@ -595,6 +602,14 @@ int ne_world_step(NeWorld* w, uint32_t nsteps) {
             ++w->stats.retries;
         }
         const neb::Ctl& c = *w->h_ctl;
+        if (w->profile) {
+            for (int k = 0; k < NE_NUM_STAGES; ++k) {
+                float ms = 0.f;
+                NE_CUDA_TRY(cudaEventElapsedTime(&ms, w->ev[k], w->ev[k + 1]));
+                w->stage_ms[k] += ms;
+            }
+            ++w->stage_steps;
+        }
         // Shrink the cell-key sort to the bits this step needed.
         if (!w->p.periodic) {
             int kb = (((int)c.need_bits + 7) / 8) * 8;
@@ -684,6 +699,29 @@ int ne_world_islands(NeWorld* w, uint32_t* label, uint32_t n) {
         label[i] = x;
     }
     return NE_OK;
+}
+
+int ne_world_profile(NeWorld* w, int enable) {
+    if (!w) return set_err(NE_ERR_ARG, "world is NULL");
+    if (enable && !w->ev[0])
+        for (int k = 0; k <= NE_NUM_STAGES; ++k) NE_CUDA_TRY(cudaEventCreate(&w->ev[k]));
+    w->profile = enable != 0;
+    for (int k = 0; k < NE_NUM_STAGES; ++k) w->stage_ms[k] = 0.0;
+    w->stage_steps = 0;
+    return NE_OK;
+}
+
+int ne_world_stage_times(NeWorld* w, double* ms, uint64_t* steps) {
+    if (!w || !ms) return set_err(NE_ERR_ARG, "NULL argument");
+    for (int k = 0; k < NE_NUM_STAGES; ++k) ms[k] = w->stage_ms[k];
+    if (steps) *steps = w->stage_steps;
+    return NE_OK;
+}
+
+const char* ne_stage_name(int k) {
+    static const char* names[NE_NUM_STAGES] = {"integrate", "broadphase", "cull", "narrowphase",
+                                               "constraints", "islands", "solve", "boundary"};
+    return (k >= 0 && k < NE_NUM_STAGES) ? names[k] : "?";
 }
 
 int ne_world_stream(const NeWorld* w, void** stream) {

@@ -773,14 +773,19 @@ inline uint32_t blocks_for(uint64_t n, int t) { return (uint32_t)((n + t - 1) / 
 
 // Enqueue one step.  The host reads ctl afterwards to learn whether it must
 // be re-run with larger buffers.
-void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches) {
+void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEvent_t* ev) {
     StepArgs a = a0;
     const DevWorld& d = a.d;
     Ctl* ctl = d.ctl;
     uint64_t& L = *launches;
+    auto mark = [&](int k) {
+        if (ev) cudaEventRecord(ev[k], st);
+    };
+    mark(0);
     k_step_begin<<<1, 1, 0, st>>>(ctl); ++L;
     k_integrate<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
 
+    mark(1);
     // Broadphase: cell keys -> stable sort -> per-body partner counts -> CSR.
     int kb = 0;
     if (!a.brute) {
@@ -793,14 +798,18 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches) {
     scan_u32(d.bcnt, d.boff, a.n, d.tsum, &ctl->P, ctl, st, launches);
     k_pair_emit<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a, kb); ++L;
 
+    mark(2);
     // Narrowphase on the pairs that survive the filters and the cull.
     k_pair_cull<<<blocks_for(a.Pcap, kT), kT, 0, st>>>(a); ++L;
     scan_u32(d.pflag, d.poff, (uint32_t)a.Pcap, d.tsum, &ctl->S, ctl, st, launches);
     k_compact<<<blocks_for(a.Pcap, kT), kT, 0, st>>>(a); ++L;
+    mark(3);
     k_narrowphase<<<blocks_for(a.Scap, 128), 128, 0, st>>>(a); ++L;
+    mark(4);
     scan_u32(d.ccnt, d.coff, (uint32_t)a.Scap, d.tsum, &ctl->C, ctl, st, launches);
     k_constraint_build<<<blocks_for(a.Scap, kT), kT, 0, st>>>(a); ++L;
 
+    mark(5);
     // Islands: label, stable sort by label, segment starts.
     k_island_label<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a); ++L;
     int lbits = 1;
@@ -811,10 +820,12 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches) {
     k_island_mark<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a, ib); ++L;
     scan_u32(d.iflag, d.ioff, (uint32_t)a.Ccap, d.tsum, &ctl->scan_total, ctl, st, launches);
     k_island_start<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a); ++L;
+    mark(6);
     k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib); ++L;
-
+    mark(7);
     k_boundary<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
     k_step_end<<<1, 1, 0, st>>>(a); ++L;
+    mark(8);
 }
 
 }  // namespace neb

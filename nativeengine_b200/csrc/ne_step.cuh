@@ -24,6 +24,7 @@ struct StepArgs {
     uint64_t Pcap, Scap, Ccap;
 };
 
-void launch_step(const StepArgs& a, cudaStream_t st, uint64_t* launches);
+// ev: NE_NUM_STAGES + 1 events recorded at the stage boundaries, or nullptr.
+void launch_step(const StepArgs& a, cudaStream_t st, uint64_t* launches, cudaEvent_t* ev);
 
 }  // namespace neb

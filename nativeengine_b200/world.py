@@ -122,6 +122,17 @@ class DeviceWorld:
         _ffi.check(self._lib.ne_world_islands(self._h, _ptr(lab), self.n), "ne_world_islands")
         return lab
 
+    def profile(self, enable: bool = True):
+        _ffi.check(self._lib.ne_world_profile(self._h, 1 if enable else 0), "ne_world_profile")
+
+    def stage_times(self) -> Dict[str, float]:
+        ms = (C.c_double * _ffi.NUM_STAGES)()
+        steps = C.c_uint64()
+        _ffi.check(self._lib.ne_world_stage_times(self._h, ms, C.byref(steps)), "ne_world_stage_times")
+        out = {self._lib.ne_stage_name(k).decode(): ms[k] for k in range(_ffi.NUM_STAGES)}
+        out["steps"] = int(steps.value)
+        return out
+
     def stream_handle(self) -> int:
         s = C.c_void_p()
         _ffi.check(self._lib.ne_world_stream(self._h, C.byref(s)), "ne_world_stream")
