@@ -65,11 +65,14 @@ struct NeWorld {
     int brute = 1;
     uint32_t nplanes = 0;
     int key_bits = 64;
+    int num_sms = 148;
     // capacities (entries)
     uint64_t Pcap = 0, Scap = 0, Ccap = 0;
     size_t nverts_alloc = 0, nnc_alloc = 0, nplanes_alloc = 0;
     std::vector<double> h_invmass;   // for upload_state packing
-    std::vector<neb::D4> stage;      // host packing buffer
+    std::vector<neb::D4> stage;      // host packing buffer (uploads)
+    neb::D4* pinned = nullptr;       // page-locked staging for per-step state traffic
+    size_t pinned_cap = 0;
     NeStepStats stats{};
     uint64_t launches = 0;
     bool has_bodies = false;
@@ -88,7 +91,7 @@ void free_body_arrays(NeWorld* w) {
     dfree(d.inert); dfree(d.geom); dfree(d.ext); dfree(d.mat); dfree(d.meta); dfree(d.vrng); dfree(d.ncrng);
     dfree(d.s_pos); dfree(d.s_quat); dfree(d.s_vel); dfree(d.s_omg); dfree(d.s_frc); dfree(d.s_trq);
     dfree(d.key[0]); dfree(d.key[1]); dfree(d.val[0]); dfree(d.val[1]);
-    dfree(d.bcnt); dfree(d.boff); dfree(d.parent);
+    dfree(d.bcnt); dfree(d.boff); dfree(d.parent); dfree(d.bdeg); dfree(d.bstart);
 }
 
 void free_pair_arrays(NeWorld* w) {
@@ -105,14 +108,16 @@ void free_con_arrays(NeWorld* w) {
     neb::DevWorld& d = w->d;
     dfree(d.ci); dfree(d.cj); dfree(d.cslot); dfree(d.con_n); dfree(d.con_ra); dfree(d.con_rb); dfree(d.con_p);
     dfree(d.con_imp); dfree(d.ilab[0]); dfree(d.ilab[1]); dfree(d.iord[0]); dfree(d.iord[1]); dfree(d.iflag);
-    dfree(d.ioff); dfree(d.istart);
+    dfree(d.ioff); dfree(d.istart); dfree(d.big); dfree(d.con_kn);
+    dfree(d.rkey[0]); dfree(d.rkey[1]); dfree(d.rval[0]); dfree(d.rval[1]); dfree(d.crank);
+    dfree(d.bcnt10); dfree(d.bq10);
 }
 
 int alloc_scratch(NeWorld* w) {
     neb::DevWorld& d = w->d;
     dfree(d.hist);
     dfree(d.tsum);
-    uint64_t sortn = std::max<uint64_t>(w->n, w->Ccap);
+    uint64_t sortn = std::max<uint64_t>(w->n, 2 * w->Ccap);
     size_t hw = neb::radix_hist_words((uint32_t)sortn);
     uint64_t scann = std::max<uint64_t>(std::max<uint64_t>(w->Pcap, w->Scap), std::max<uint64_t>(hw, sortn));
     int rc;
@@ -153,7 +158,11 @@ int alloc_cons(NeWorld* w, uint64_t cap) {
         (rc = dalloc(&d.con_n, cap)) || (rc = dalloc(&d.con_ra, cap)) || (rc = dalloc(&d.con_rb, cap)) ||
         (rc = dalloc(&d.con_p, cap)) || (rc = dalloc(&d.con_imp, cap)) || (rc = dalloc(&d.ilab[0], cap)) ||
         (rc = dalloc(&d.ilab[1], cap)) || (rc = dalloc(&d.iord[0], cap)) || (rc = dalloc(&d.iord[1], cap)) ||
-        (rc = dalloc(&d.iflag, cap)) || (rc = dalloc(&d.ioff, cap)) || (rc = dalloc(&d.istart, cap + 1)))
+        (rc = dalloc(&d.iflag, cap)) || (rc = dalloc(&d.ioff, cap)) || (rc = dalloc(&d.istart, cap + 1)) ||
+        (rc = dalloc(&d.big, cap)) || (rc = dalloc(&d.con_kn, cap)) || (rc = dalloc(&d.rkey[0], 2 * cap)) ||
+        (rc = dalloc(&d.rkey[1], 2 * cap)) || (rc = dalloc(&d.rval[0], 2 * cap)) ||
+        (rc = dalloc(&d.rval[1], 2 * cap)) || (rc = dalloc(&d.crank, 2 * cap)) ||
+        (rc = dalloc(&d.bcnt10, 10 * cap)) || (rc = dalloc(&d.bq10, 10 * cap)))
         return rc;
     unsigned long long* nk[2] = {nullptr, nullptr};
     double* ni[2] = {nullptr, nullptr};
@@ -203,6 +212,7 @@ neb::StepArgs make_args(const NeWorld* w) {
     a.Pcap = w->Pcap;
     a.Scap = w->Scap;
     a.Ccap = w->Ccap;
+    a.num_sms = w->num_sms;
     return a;
 }
 
@@ -303,6 +313,7 @@ int ne_world_create(const NeWorldParams* params, NeWorld** out) {
     NeWorld* w = new NeWorld();
     w->p = *params;
     NE_CUDA_TRY(cudaGetDevice(&w->device));
+    NE_CUDA_TRY(cudaDeviceGetAttribute(&w->num_sms, cudaDevAttrMultiProcessorCount, w->device));
     NE_CUDA_TRY(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
     NE_CUDA_TRY(cudaMallocHost((void**)&w->h_ctl, sizeof(neb::Ctl)));
     if ((rc = dalloc(&w->d.ctl, 1))) { ne_world_destroy(w); return rc; }
@@ -324,6 +335,7 @@ int ne_world_destroy(NeWorld* w) {
     for (int b = 0; b < 2; ++b) { dfree(d.wkey[b]); dfree(d.wimp[b]); }
     dfree(d.hist); dfree(d.tsum); dfree(d.ctl);
     if (w->h_ctl) cudaFreeHost(w->h_ctl);
+    if (w->pinned) cudaFreeHost(w->pinned);
     for (int k = 0; k <= NE_NUM_STAGES; ++k)
         if (w->ev[k]) cudaEventDestroy(w->ev[k]);
     if (w->stream) cudaStreamDestroy(w->stream);
@@ -395,7 +407,8 @@ int ne_world_upload(NeWorld* w, const NeBodyArrays* b) {
             (rc = dalloc(&d.s_vel, m)) || (rc = dalloc(&d.s_omg, m)) || (rc = dalloc(&d.s_frc, m)) ||
             (rc = dalloc(&d.s_trq, m)) || (rc = dalloc(&d.key[0], m)) || (rc = dalloc(&d.key[1], m)) ||
             (rc = dalloc(&d.val[0], m)) || (rc = dalloc(&d.val[1], m)) || (rc = dalloc(&d.bcnt, m)) ||
-            (rc = dalloc(&d.boff, m)) || (rc = dalloc(&d.parent, m)))
+            (rc = dalloc(&d.boff, m)) || (rc = dalloc(&d.parent, m)) || (rc = dalloc(&d.bdeg, m)) ||
+            (rc = dalloc(&d.bstart, m)))
             return rc;
     }
     // Pack the host arrays into the 32-byte device records.
@@ -491,34 +504,50 @@ int ne_world_upload(NeWorld* w, const NeBodyArrays* b) {
     return NE_OK;
 }
 
+// Pinned host staging for per-step state traffic: 6 records per body
+// (pos, quat, vel, omg, frc, trq), so each transfer is one async copy per
+// array straight from page-locked memory.
+static int ensure_pinned(NeWorld* w) {
+    const size_t need = (size_t)6 * (w->n ? w->n : 1);
+    if (w->pinned_cap >= need) return NE_OK;
+    if (w->pinned) cudaFreeHost(w->pinned);
+    w->pinned = nullptr;
+    w->pinned_cap = 0;
+    NE_CUDA_TRY(cudaMallocHost((void**)&w->pinned, need * sizeof(neb::D4)));
+    w->pinned_cap = need;
+    return NE_OK;
+}
+
 int ne_world_upload_state(NeWorld* w, const double* x, const double* q, const double* v, const double* wv) {
     if (!w || !w->has_bodies) return set_err(NE_ERR_ARG, "world has no bodies");
     const uint32_t n = w->n;
     if (!n) return NE_OK;
-    std::vector<neb::D4>& st = w->stage;
-    st.resize(n);
-    auto put = [&](neb::D4* dst) -> int {
-        cudaError_t e = cudaMemcpyAsync(dst, st.data(), n * sizeof(neb::D4), cudaMemcpyHostToDevice, w->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
-        return e == cudaSuccess ? NE_OK : set_err(NE_ERR_CUDA, cudaGetErrorString(e));
-    };
     int rc;
+    if ((rc = ensure_pinned(w))) return rc;
+    neb::D4* st = w->pinned;
+    const size_t bytes = (size_t)n * sizeof(neb::D4);
     if (x) {
-        for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{x[3 * i], x[3 * i + 1], x[3 * i + 2], w->h_invmass[i]};
-        if ((rc = put(w->d.pos))) return rc;
+        neb::D4* s = st;
+        for (uint32_t i = 0; i < n; ++i) s[i] = neb::D4{x[3 * i], x[3 * i + 1], x[3 * i + 2], w->h_invmass[i]};
+        NE_CUDA_TRY(cudaMemcpyAsync(w->d.pos, s, bytes, cudaMemcpyHostToDevice, w->stream));
     }
     if (q) {
-        for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]};
-        if ((rc = put(w->d.quat))) return rc;
+        neb::D4* s = st + n;
+        for (uint32_t i = 0; i < n; ++i) s[i] = neb::D4{q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]};
+        NE_CUDA_TRY(cudaMemcpyAsync(w->d.quat, s, bytes, cudaMemcpyHostToDevice, w->stream));
     }
     if (v) {
-        for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0};
-        if ((rc = put(w->d.vel))) return rc;
+        neb::D4* s = st + 2 * (size_t)n;
+        for (uint32_t i = 0; i < n; ++i) s[i] = neb::D4{v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0};
+        NE_CUDA_TRY(cudaMemcpyAsync(w->d.vel, s, bytes, cudaMemcpyHostToDevice, w->stream));
     }
     if (wv) {
-        for (uint32_t i = 0; i < n; ++i) st[i] = neb::D4{wv[3 * i], wv[3 * i + 1], wv[3 * i + 2], 0.0};
-        if ((rc = put(w->d.omg))) return rc;
+        neb::D4* s = st + 3 * (size_t)n;
+        for (uint32_t i = 0; i < n; ++i) s[i] = neb::D4{wv[3 * i], wv[3 * i + 1], wv[3 * i + 2], 0.0};
+        NE_CUDA_TRY(cudaMemcpyAsync(w->d.omg, s, bytes, cudaMemcpyHostToDevice, w->stream));
     }
+    // The staging buffer is reused by the next call: wait for the copies.
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
     return NE_OK;
 }
 
@@ -527,28 +556,25 @@ int ne_world_download(NeWorld* w, NeBodyArrays* out) {
     if (!w->has_bodies) return set_err(NE_ERR_ARG, "world has no bodies");
     const uint32_t n = std::min(w->n, out->n);
     if (!n) return NE_OK;
-    std::vector<neb::D4>& st = w->stage;
-    st.resize(w->n);
-    auto get = [&](const neb::D4* src) -> int {
-        cudaError_t e = cudaMemcpyAsync(st.data(), src, n * sizeof(neb::D4), cudaMemcpyDeviceToHost, w->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
-        return e == cudaSuccess ? NE_OK : set_err(NE_ERR_CUDA, cudaGetErrorString(e));
-    };
     int rc;
-    auto unpack3 = [&](double* dst) {
-        for (uint32_t i = 0; i < n; ++i) { dst[3 * i] = st[i].x; dst[3 * i + 1] = st[i].y; dst[3 * i + 2] = st[i].z; }
-    };
-    if (out->x) { if ((rc = get(w->d.pos))) return rc; unpack3(out->x); }
-    if (out->q) {
-        if ((rc = get(w->d.quat))) return rc;
-        for (uint32_t i = 0; i < n; ++i) {
-            out->q[4 * i] = st[i].x; out->q[4 * i + 1] = st[i].y; out->q[4 * i + 2] = st[i].z; out->q[4 * i + 3] = st[i].w;
+    if ((rc = ensure_pinned(w))) return rc;
+    neb::D4* st = w->pinned;
+    const size_t bytes = (size_t)n * sizeof(neb::D4);
+    const neb::D4* src[6] = {w->d.pos, w->d.quat, w->d.vel, w->d.omg, w->d.frc, w->d.trq};
+    double* dst[6] = {out->x, out->q, out->v, out->w, out->force, out->torque};
+    for (int k = 0; k < 6; ++k)
+        if (dst[k]) NE_CUDA_TRY(cudaMemcpyAsync(st + (size_t)k * n, src[k], bytes, cudaMemcpyDeviceToHost, w->stream));
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    for (int k = 0; k < 6; ++k) {
+        if (!dst[k]) continue;
+        const neb::D4* s = st + (size_t)k * n;
+        double* o = dst[k];
+        if (k == 1) {
+            for (uint32_t i = 0; i < n; ++i) { o[4 * i] = s[i].x; o[4 * i + 1] = s[i].y; o[4 * i + 2] = s[i].z; o[4 * i + 3] = s[i].w; }
+        } else {
+            for (uint32_t i = 0; i < n; ++i) { o[3 * i] = s[i].x; o[3 * i + 1] = s[i].y; o[3 * i + 2] = s[i].z; }
         }
     }
-    if (out->v) { if ((rc = get(w->d.vel))) return rc; unpack3(out->v); }
-    if (out->w) { if ((rc = get(w->d.omg))) return rc; unpack3(out->w); }
-    if (out->force) { if ((rc = get(w->d.frc))) return rc; unpack3(out->force); }
-    if (out->torque) { if ((rc = get(w->d.trq))) return rc; unpack3(out->torque); }
     return NE_OK;
 }
 
@@ -622,6 +648,7 @@ int ne_world_step(NeWorld* w, uint32_t nsteps) {
         w->stats.max_island = c.max_island;
         w->stats.epa_cap_hits += c.epa_cap_hits;
         w->stats.steps += 1;
+        if (c.solve_timeout) return set_err(NE_ERR_TIMEOUT, "a dataflow-solver dependency wait ran out");
         if (c.flags & 1u) status = set_err(NE_ERR_NUMERIC, "an EPA or clipping budget was exceeded");
     }
     return status;

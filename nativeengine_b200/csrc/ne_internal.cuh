@@ -38,6 +38,8 @@ struct Ctl {
     uint32_t wsel;           // warm cache buffer holding the previous step
     uint64_t P, S, C;        // pairs, survivors, contacts (totals, even if over capacity)
     uint64_t islands, max_island, epa_cap_hits;
+    uint32_t nbig;           // islands solved by the dataflow kernel this step
+    uint32_t solve_timeout;  // a bounded dependency wait ran out (error)
     uint32_t wcount[2];      // warm cache entries per buffer
     long long cmin[3], cmax[3];   // cell coordinate extents (open/reflective grid)
     uint64_t scan_total;     // scratch total of the last scan
@@ -78,6 +80,15 @@ struct DevWorld {
     uint32_t* parent;
     uint32_t *ilab[2], *iord[2];
     uint32_t *iflag, *ioff, *istart;
+    uint32_t* big;           // islands handed to the dataflow solver
+    double* con_kn;          // effective mass along n (constant during the solve)
+    // per-body update ranks for the dataflow solver
+    uint32_t *rkey[2], *rval[2];   // (body, 2*position+side) entries, 2 per contact
+    uint32_t* crank;         // [2C] rank of each contact among its body's contacts
+    uint32_t* bdeg;          // [n] contacts per body in its island
+    uint32_t* bstart;        // [n] first rank entry of each body in the sorted entries
+    uint32_t* bcnt10;        // [10C] unfinished-predecessor counts of the solver updates
+    uint32_t* bq10;          // [10C] ready queues of the solver updates
     // scratch
     uint32_t *hist, *tsum;
     Ctl* ctl;

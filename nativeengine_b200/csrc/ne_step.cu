@@ -8,12 +8,14 @@
 //   constraint build       src/world.cpp:537-553   k_constraint_build (+ union-find hooking)
 //   islands                src/world.cpp:332-343   k_island_label, radix sort, k_island_mark/_start
 //   warm start + 8 SI + position correction + warm-cache store
-//                          src/world.cpp:559-626   k_island_solve
+//                          src/world.cpp:559-626   k_island_solve, k_island_solve_big
 //   wrapPositions/applyWalls src/world.cpp:635-702 k_boundary
 //
 // Every kernel is a no-op once ctl->abort is set (a capacity overflow this
 // step); the host then restores the pre-step snapshot, grows the buffer and
 // re-runs the step, so an overflow never changes the result.
+#include <cuda/atomic>
+
 #include "ne_step.cuh"
 
 namespace neb {
@@ -155,6 +157,8 @@ __global__ void k_step_begin(Ctl* ctl) {
     ctl->islands = 0;
     ctl->max_island = 0;
     ctl->epa_cap_hits = 0;
+    ctl->nbig = 0;
+    ctl->solve_timeout = 0;
     for (int a = 0; a < 3; ++a) {
         ctl->cmin[a] = 0x7fffffffffffffffll;
         ctl->cmax[a] = (long long)0x8000000000000000ull;
@@ -288,9 +292,12 @@ __global__ void __launch_bounds__(kT) k_pair_count(StepArgs a, int kb) {
     d.bcnt[i] = cnt;
 }
 
-// Writes body i's sorted partner list at its CSR offset.  One warp per body:
-// lanes 0..26 own one neighbour cell run each, lane 27 the plane list; every
-// partner's output rank is the number of smaller partners over all runs.
+// Writes body i's sorted partner list at its CSR offset.  One warp per body.
+// The partner candidates are up to 27 sorted runs (one per distinct
+// neighbour cell; members with index > i) plus the sorted run of planes > i.
+// Lanes split the concatenated candidates evenly; each candidate's output rank
+// is its index in its own run plus the number of smaller candidates in the
+// other runs (all candidates are distinct body indices).
 __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
@@ -298,7 +305,8 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
         if (threadIdx.x == 0 && blockIdx.x == 0) ctl->abort = 1;
         return;
     }
-    const int lane = threadIdx.x & 31;
+    __shared__ uint32_t s_lo[kT / 32][28], s_len[kT / 32][28], s_ex[kT / 32][29];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= a.n) return;
     const DevWorld& d = a.d;
@@ -316,10 +324,9 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
     const long long cx = cell_of(a, p.x, 0), cy = cell_of(a, p.y, 1), cz = cell_of(a, p.z, 2);
     const unsigned long long* keys = d.key[kb];
     const uint32_t* vals = d.val[kb];
-    // Lane t < 27 takes neighbour offset t; duplicates (wrap aliasing) keep
-    // only their lowest lane.
+    // Lane t < 27 takes neighbour offset t (duplicates from wrap aliasing keep
+    // their lowest lane); lane 27 takes the plane list.
     uint32_t rlo = 0, rhi = 0;
-    const uint32_t* src = vals;
     if (lane < 27) {
         const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
         unsigned long long k = compact_key(L, wrap_cell(a, cx + dx, 0), wrap_cell(a, cy + dy, 1),
@@ -332,33 +339,52 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
             rhi = hi;
         }
     } else if (lane == 27) {
-        src = d.planes;
         rlo = upper_bound_u32(d.planes, 0, a.nplanes, i);
         rhi = a.nplanes;
     }
+    // Compact the non-empty runs into shared memory, in lane order.
     const uint32_t len = rhi - rlo;
-    // Each lane walks the elements of its own run; the rank of element x is
-    // its index in its run plus the count of smaller elements in other runs.
-    for (uint32_t e = 0;; ++e) {   // ends after the longest run (at most n - 1 rounds)
-        // Round e: every lane takes the e-th element of its run, if any.
-        const bool has = e < len;
-        if (!__any_sync(0xffffffffu, has)) break;
-        uint32_t x = has ? src[rlo + e] : 0u;
-        uint32_t rank = e;
-        // Count elements < x in the other lanes' runs.
-        for (int r = 0; r < 28; ++r) {
-            const uint32_t olo = __shfl_sync(0xffffffffu, rlo, r);
-            const uint32_t ohi = __shfl_sync(0xffffffffu, rhi, r);
-            if (r == lane || !has || olo == ohi) continue;
-            const uint32_t* os = (r == 27) ? d.planes : vals;
-            rank += lower_bound_u32(os, olo, ohi, x) - olo;
+    const uint32_t nonempty = __ballot_sync(0xffffffffu, len > 0);
+    const int r = __popc(nonempty & ((1u << lane) - 1u));
+    uint32_t incl = len;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const int nr = __popc(nonempty);
+    // The plane run (lane 27) is the last non-empty run if present.
+    const bool planes_nonempty = (nonempty >> 27) & 1u;
+    if (len > 0) {
+        s_lo[wid][r] = rlo;
+        s_len[wid][r] = len;
+        s_ex[wid][r] = incl - len;
+    }
+    if (lane == 0) s_ex[wid][nr] = total;
+    __syncwarp();
+    for (uint32_t e = lane; e < total; e += 32) {
+        // Owning run: last r with s_ex[r] <= e.
+        int lo = 0, hi = nr - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (s_ex[wid][mid] <= e) lo = mid; else hi = mid - 1;
         }
-        if (has) {
-            d.pair_i[base + rank] = i;
-            d.pair_j[base + rank] = x;
+        const int own = lo;
+        const uint32_t idx = e - s_ex[wid][own];
+        const bool own_plane = planes_nonempty && own == nr - 1;
+        const uint32_t x = own_plane ? d.planes[s_lo[wid][own] + idx] : vals[s_lo[wid][own] + idx];
+        uint32_t rank = idx;
+        for (int q = 0; q < nr; ++q) {
+            if (q == own) continue;
+            const uint32_t ql = s_lo[wid][q], qh = ql + s_len[wid][q];
+            const uint32_t* src = (planes_nonempty && q == nr - 1) ? d.planes : vals;
+            rank += lower_bound_u32(src, ql, qh, x) - ql;
         }
+        d.pair_i[base + rank] = i;
+        d.pair_j[base + rank] = x;
     }
 }
+
 
 // Pair filters (src/world.cpp:513-516) and a conservative bounding-volume cull
 // that only removes pairs the narrowphase provably reports as separated.
@@ -495,6 +521,16 @@ __device__ __forceinline__ void uf_union(uint32_t* parent, uint32_t a, uint32_t 
     }
 }
 
+// effMass(a, b, rA, rB, u) (src/contact.hpp:28-33) from the body arrays.
+__device__ __forceinline__ double eff_mass_at(const DevWorld& d, uint32_t i, uint32_t j, const V3& ra, const V3& rb,
+                                              const V3& u) {
+    const Q qa = qof(d.quat[i]), qb = qof(d.quat[j]);
+    const V3 ia = v3of(d.inert[i]), ibv = v3of(d.inert[j]);
+    V3 angA = cross(apply_inv_inertia(qa, ia, cross(ra, u)), ra);
+    V3 angB = cross(apply_inv_inertia(qb, ibv, cross(rb, u)), rb);
+    return d.pos[i].w + d.pos[j].w + dot(angA + angB, u);
+}
+
 // Contact constraints of one surviving pair (src/world.cpp:518-553): lever
 // arms, restitution bias from the pre-solve velocities, combined material,
 // warm-start impulse looked up in the previous step's sorted cache.
@@ -547,6 +583,7 @@ __global__ void __launch_bounds__(kT) k_constraint_build(StepArgs a) {
         d.con_rb[c] = d4of(rB, mu);
         d.con_p[c] = d4of(pt, 0.0);
         d.con_imp[c] = make_double2(nImp, 0.0);
+        d.con_kn[c] = eff_mass_at(d, i, j, rA, rB, n);
         d.wkey[ws ^ 1][c] = key;
     }
 }
@@ -579,6 +616,10 @@ __global__ void __launch_bounds__(kT) k_island_mark(StepArgs a, int ib) {
     a.d.iflag[k] = f;
 }
 
+// Island segments; islands with at least kBigIsland contacts are queued for
+// the dataflow solver, the rest are solved one thread per island.
+constexpr uint32_t kBigIsland = 48;
+
 __global__ void __launch_bounds__(kT) k_island_start(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
@@ -589,6 +630,50 @@ __global__ void __launch_bounds__(kT) k_island_start(StepArgs a) {
         a.d.istart[ctl->scan_total] = (uint32_t)C;
     }
     if (k < C && a.d.iflag[k]) a.d.istart[a.d.ioff[k]] = (uint32_t)k;
+}
+
+// Per-body rank entries: for every contact position p (island order) and each
+// mutable endpoint, key = body, value = 2p + side.  Padding sorts last.
+__global__ void __launch_bounds__(kT) k_rank_entries(StepArgs a, int ib) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.Ccap) return;
+    const DevWorld& d = a.d;
+    uint32_t ka = a.n, kb = a.n;
+    if (p < ctl->C) {
+        const uint32_t c = d.iord[ib][p];
+        const uint32_t i = d.ci[c], j = d.cj[c];
+        if (d.meta[i].y & kFlagMutable) ka = i;
+        if (d.meta[j].y & kFlagMutable) kb = j;
+    }
+    d.rkey[0][2 * p] = ka;
+    d.rval[0][2 * p] = (uint32_t)(2 * p);
+    d.rkey[0][2 * p + 1] = kb;
+    d.rval[0][2 * p + 1] = (uint32_t)(2 * p + 1);
+}
+
+// After the stable sort by body: rank = index within the body's run, the run
+// start and length are the body's first entry and contact count.
+__global__ void __launch_bounds__(kT) k_rank_write(StepArgs a, int rb) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t E = 2 * a.Ccap;
+    if (e >= E) return;
+    const DevWorld& d = a.d;
+    const uint32_t* key = d.rkey[rb];
+    const uint32_t body = key[e];
+    if (body >= a.n) return;
+    const uint32_t v = d.rval[rb][e];
+    uint32_t lo = 0, hi = (uint32_t)e;   // run start: first index with this key
+    while (lo < hi) {
+        uint32_t mid = lo + ((hi - lo) >> 1);
+        if (key[mid] < body) lo = mid + 1; else hi = mid;
+    }
+    d.crank[v] = (uint32_t)e - lo;
+    if (e == lo) d.bstart[body] = lo;
+    if (e + 1 == E || key[e + 1] != body) d.bdeg[body] = (uint32_t)e - lo + 1;
 }
 
 struct BodyS {
@@ -632,11 +717,82 @@ __device__ __forceinline__ void store_solver_body(const DevWorld& d, uint32_t i,
     d.omg[i] = d4of(b.w, 0.0);
 }
 
-// One thread per island: warm start (src/world.cpp:559-568), 8 Gauss-Seidel
-// sweeps in the reference's constraint order (:572-612), position correction
-// (:615-616), and the impulses for the warm-cache store (:619-626).  Islands
-// share no mutable body, so running them concurrently reproduces the
-// reference's single global sweep exactly.
+// Warm-start application of one contact (src/world.cpp:560-567).
+__device__ __forceinline__ void warm_item(const DevWorld& d, uint32_t c) {
+    const double nImp = d.con_imp[c].x;
+    if (nImp == 0.0) return;
+    const uint32_t i = d.ci[c], j = d.cj[c];
+    BodyS A = load_solver_body(d, i), B = load_solver_body(d, j);
+    const V3 n = v3of(d.con_n[c]), rA = v3of(d.con_ra[c]), rB = v3of(d.con_rb[c]);
+    apply_pair_impulse(A, B, rA, rB, n * nImp);
+    store_solver_body(d, i, A);
+    store_solver_body(d, j, B);
+}
+
+// One sequential-impulse update of one contact (src/world.cpp:575-610).  Kn
+// is the effMass along n computed once at constraint build: the reference
+// recomputes it every sweep from the same (unchanged) operands, so the value
+// is identical.
+__device__ __forceinline__ void sweep_item(const DevWorld& d, uint32_t c) {
+    const uint32_t i = d.ci[c], j = d.cj[c];
+    BodyS A = load_solver_body(d, i), B = load_solver_body(d, j);
+    const D4 cn = d.con_n[c], ra4 = d.con_ra[c], rb4 = d.con_rb[c];
+    const V3 n = v3of(cn), rA = v3of(ra4), rB = v3of(rb4);
+    const double restBias = ra4.w, mu = rb4.w;
+    const double Kn = d.con_kn[c];
+    double2 imp = d.con_imp[c];
+    const V3 vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+    const double vn = dot(vc, n);
+    if (Kn > 1e-18) {
+        double dj = (restBias - vn) / Kn;
+        const double old = imp.x;
+        imp.x = (old + dj > 0.0) ? old + dj : 0.0;
+        dj = imp.x - old;
+        apply_pair_impulse(A, B, rA, rB, n * dj);
+    }
+    if (mu > 0.0 && imp.x > 0.0) {
+        const V3 vc2 = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+        const V3 vt = vc2 - n * dot(vc2, n);
+        const double vtl = norm(vt);
+        if (vtl > 1e-12) {
+            const V3 tg = vt / vtl;
+            const double Kt = eff_mass(A, B, rA, rB, tg);
+            if (Kt > 1e-18) {
+                double djt = -vtl / Kt;
+                const double maxF = mu * imp.x;
+                const double old = imp.y;
+                const double sum = old + djt;
+                imp.y = (sum < -maxF) ? -maxF : (sum > maxF ? maxF : sum);
+                djt = imp.y - old;
+                apply_pair_impulse(A, B, rA, rB, tg * djt);
+            }
+        }
+    }
+    d.con_imp[c] = imp;
+    store_solver_body(d, i, A);
+    store_solver_body(d, j, B);
+}
+
+// correctPenetration (src/contact.hpp:78-85) and the warm-cache store value.
+__device__ __forceinline__ void correct_item(const DevWorld& d, uint32_t c, double beta, double* wimp_out) {
+    const uint32_t i = d.ci[c], j = d.cj[c];
+    const D4 pa = d.pos[i], pb = d.pos[j];
+    const double invSum = pa.w + pb.w;
+    const D4 cn = d.con_n[c];
+    const double overlap = cn.w;
+    if (!(invSum <= 0.0 || overlap <= 0.0)) {
+        const V3 corr = v3of(cn) * (beta * overlap / invSum);
+        if (d.meta[i].y & kFlagMutable) d.pos[i] = d4of(v3of(pa) + corr * pa.w, pa.w);
+        if (d.meta[j].y & kFlagMutable) d.pos[j] = d4of(v3of(pb) - corr * pb.w, pb.w);
+    }
+    if (wimp_out) wimp_out[c] = d.con_imp[c].x;
+}
+
+// One thread per small island: warm start (src/world.cpp:559-568), 8
+// Gauss-Seidel sweeps in the reference's contact order (:572-612), position
+// correction (:615-616), warm-cache values (:619-626).  Islands share no
+// mutable body, so concurrent islands reproduce the reference's single
+// global sweep exactly.  Big islands are queued for k_island_solve_big.
 __global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
@@ -644,78 +800,158 @@ __global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
     if (t >= ctl->islands) return;
     const DevWorld& d = a.d;
     const uint32_t s = d.istart[t], e = d.istart[t + 1];
-    const uint32_t* ord = d.iord[ib];
     atomicMax((unsigned long long*)&ctl->max_island, (unsigned long long)(e - s));
+    if (e - s >= kBigIsland) {
+        const uint32_t slot = atomicAdd(&ctl->nbig, 1u);
+        d.big[slot] = (uint32_t)t;
+        return;
+    }
+    const uint32_t* ord = d.iord[ib];
+    if (a.warm)
+        for (uint32_t k = s; k < e; ++k) warm_item(d, ord[k]);
+    for (int it = 0; it < 8; ++it)
+        for (uint32_t k = s; k < e; ++k) sweep_item(d, ord[k]);
+    double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
+    for (uint32_t k = s; k < e; ++k) correct_item(d, ord[k], a.beta, wout);
+}
 
-    if (a.warm) {
-        for (uint32_t k = s; k < e; ++k) {
-            const uint32_t c = ord[k];
-            const double nImp = d.con_imp[c].x;
-            if (nImp == 0.0) continue;
-            const uint32_t i = d.ci[c], j = d.cj[c];
-            BodyS A = load_solver_body(d, i), B = load_solver_body(d, j);
-            const V3 n = v3of(d.con_n[c]), rA = v3of(d.con_ra[c]), rB = v3of(d.con_rb[c]);
-            apply_pair_impulse(A, B, rA, rB, n * nImp);
-            store_solver_body(d, i, A);
-            store_solver_body(d, j, B);
+constexpr uint32_t kRoundLimit = 1u << 26;
+constexpr uint32_t kEmpty = 0xffffffffu;
+constexpr int kBigThreads = 512;
+
+// Island-local view of one contact's update (phase p, contact position pos).
+struct BigItem {
+    uint32_t c, i, j, pos, p;
+    bool mi, mj;
+};
+
+__device__ __forceinline__ BigItem big_item(const DevWorld& d, const uint32_t* ord, uint32_t s, uint32_t m,
+                                            uint32_t u) {
+    BigItem it;
+    it.p = u / m;
+    it.pos = s + (u - it.p * m);
+    it.c = ord[it.pos];
+    it.i = d.ci[it.c];
+    it.j = d.cj[it.c];
+    it.mi = (d.meta[it.i].y & kFlagMutable) != 0;
+    it.mj = (d.meta[it.j].y & kFlagMutable) != 0;
+    return it;
+}
+
+// Number of earlier updates this update waits for: one per mutable body,
+// except a body's very first update (phase 0, rank 0).
+__device__ __forceinline__ uint32_t big_npred(const DevWorld& d, const BigItem& it) {
+    uint32_t n = 0;
+    if (it.mi && !(it.p == 0 && d.crank[2 * it.pos] == 0)) ++n;
+    if (it.mj && !(it.p == 0 && d.crank[2 * it.pos + 1] == 0)) ++n;
+    return n;
+}
+
+// The update that follows this one on body b (side 0 = i, 1 = j), or kEmpty.
+__device__ __forceinline__ uint32_t big_successor(const DevWorld& d, const uint32_t* rv, const BigItem& it, int side,
+                                                  uint32_t b, uint32_t s, uint32_t m) {
+    const uint32_t r = d.crank[2 * it.pos + side];
+    const uint32_t deg = d.bdeg[b];
+    const uint32_t base = d.bstart[b];
+    if (r + 1 < deg) return it.p * m + ((rv[base + r + 1] >> 1) - s);
+    if (it.p < 9) return (it.p + 1) * m + ((rv[base] >> 1) - s);
+    return kEmpty;
+}
+
+__device__ __forceinline__ void big_push(uint32_t* queue, uint32_t* tail, uint32_t u) {
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> t(*tail);
+    const uint32_t slot = t.fetch_add(1u, cuda::memory_order_relaxed);
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> q(queue[slot]);
+    q.store(u, cuda::memory_order_release);
+}
+
+__device__ __forceinline__ void big_notify(uint32_t* cnt, uint32_t* queue, uint32_t* tail, uint32_t u) {
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> c(cnt[u]);
+    if (c.fetch_sub(1u, cuda::memory_order_acq_rel) == 1u) big_push(queue, tail, u);
+}
+
+// Dataflow solver for the big islands, one CTA per island.
+//
+// The reference's work on an island is a sequence of 10*m updates (phase 0 =
+// warm start, phases 1-8 = the Gauss-Seidel sweeps, phase 9 = position
+// correction; m contacts in order).  An update reads and writes only its two
+// bodies, so it depends only on the previous update of each of those bodies
+// in that sequence.  Each update counts its unfinished predecessors (<= 2);
+// finishing an update decrements its successors' counts, and the update that
+// reaches zero is appended to a ready queue.  Lanes claim queue slots in order
+// and run the update in a slot once it is filled.  Every body therefore sees
+// exactly the reference's sequence of updates (bit-identical result), and the
+// schedule is greedy list scheduling, whose length is close to the
+// dependency graph's critical path.  Progress is guaranteed: while updates
+// remain, some update is ready, and the lowest unfilled slot is claimed by a
+// waiting lane.  Lanes poll warp-synchronously (no lane spins alone, so a
+// ready update is never starved by divergent waiters), and every wait is
+// bounded and reports through ctl->solve_timeout.
+__global__ void __launch_bounds__(kBigThreads) k_island_solve_big(StepArgs a, int ib, int rb) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    __shared__ int s_fail;
+    __shared__ uint32_t s_head, s_tail;
+    const DevWorld& d = a.d;
+    const uint32_t* ord = d.iord[ib];
+    const uint32_t* rv = d.rval[rb];
+    double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
+    const uint32_t nbig = ctl->nbig;
+    for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+        const uint32_t t = d.big[bi];
+        const uint32_t s = d.istart[t], e = d.istart[t + 1];
+        const uint32_t m = e - s;
+        const uint32_t total = 10u * m;
+        uint32_t* cnt = d.bcnt10 + 10u * s;      // per-island slices of the 10*C scratch
+        uint32_t* queue = d.bq10 + 10u * s;
+        if (threadIdx.x == 0) { s_fail = 0; s_head = 0; s_tail = 0; }
+        for (uint32_t u = threadIdx.x; u < total; u += blockDim.x) {
+            cnt[u] = big_npred(d, big_item(d, ord, s, m, u));
+            queue[u] = kEmpty;
         }
-    }
-    for (int it = 0; it < 8; ++it) {
-        for (uint32_t k = s; k < e; ++k) {
-            const uint32_t c = ord[k];
-            const uint32_t i = d.ci[c], j = d.cj[c];
-            BodyS A = load_solver_body(d, i), B = load_solver_body(d, j);
-            const D4 cn = d.con_n[c], ra4 = d.con_ra[c], rb4 = d.con_rb[c];
-            const V3 n = v3of(cn), rA = v3of(ra4), rB = v3of(rb4);
-            const double restBias = ra4.w, mu = rb4.w;
-            double2 imp = d.con_imp[c];
-            const V3 vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
-            const double vn = dot(vc, n);
-            const double Kn = eff_mass(A, B, rA, rB, n);
-            if (Kn > 1e-18) {
-                double dj = (restBias - vn) / Kn;
-                const double old = imp.x;
-                imp.x = (old + dj > 0.0) ? old + dj : 0.0;
-                dj = imp.x - old;
-                apply_pair_impulse(A, B, rA, rB, n * dj);
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x)
+            if (cnt[k] == 0) big_push(queue, &s_tail, k);
+        __syncthreads();
+
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_block> head(s_head);
+        uint32_t h = head.fetch_add(1u, cuda::memory_order_relaxed);
+        uint32_t idle = 0;
+        while (true) {
+            const bool live = h < total;
+            if (!__any_sync(0xffffffffu, live)) break;
+            uint32_t u = kEmpty;
+            if (live) {
+                cuda::atomic_ref<uint32_t, cuda::thread_scope_block> q(queue[h]);
+                u = q.load(cuda::memory_order_acquire);
             }
-            if (mu > 0.0 && imp.x > 0.0) {
-                const V3 vc2 = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
-                const V3 vt = vc2 - n * dot(vc2, n);
-                const double vtl = norm(vt);
-                if (vtl > 1e-12) {
-                    const V3 tg = vt / vtl;
-                    const double Kt = eff_mass(A, B, rA, rB, tg);
-                    if (Kt > 1e-18) {
-                        double djt = -vtl / Kt;
-                        const double maxF = mu * imp.x;
-                        const double old = imp.y;
-                        const double sum = old + djt;
-                        imp.y = (sum < -maxF) ? -maxF : (sum > maxF ? maxF : sum);
-                        djt = imp.y - old;
-                        apply_pair_impulse(A, B, rA, rB, tg * djt);
-                    }
+            const bool ready = u != kEmpty;
+            if (ready) {
+                const BigItem it = big_item(d, ord, s, m, u);
+                if (it.p == 0) {
+                    if (a.warm) warm_item(d, it.c);
+                } else if (it.p <= 8) {
+                    sweep_item(d, it.c);
+                } else {
+                    correct_item(d, it.c, a.beta, wout);
                 }
+                const uint32_t si = it.mi ? big_successor(d, rv, it, 0, it.i, s, m) : kEmpty;
+                const uint32_t sj = it.mj ? big_successor(d, rv, it, 1, it.j, s, m) : kEmpty;
+                if (si != kEmpty) big_notify(cnt, queue, &s_tail, si);
+                if (sj != kEmpty) big_notify(cnt, queue, &s_tail, sj);
+                h = head.fetch_add(1u, cuda::memory_order_relaxed);
             }
-            d.con_imp[c] = imp;
-            store_solver_body(d, i, A);
-            store_solver_body(d, j, B);
+            idle = __any_sync(0xffffffffu, ready) ? 0u : idle + 1u;
+            const bool failed = __any_sync(0xffffffffu, *(volatile int*)&s_fail != 0);   // warp-uniform
+            if (idle > kRoundLimit || failed) {
+                if ((threadIdx.x & 31) == 0) {
+                    s_fail = 1;
+                    atomicExch(&ctl->solve_timeout, 1u);
+                }
+                break;
+            }
         }
-    }
-    // correctPenetration (src/contact.hpp:78-85), in constraint order.
-    for (uint32_t k = s; k < e; ++k) {
-        const uint32_t c = ord[k];
-        const uint32_t i = d.ci[c], j = d.cj[c];
-        const D4 pa = d.pos[i], pb = d.pos[j];
-        const double invSum = pa.w + pb.w;
-        const D4 cn = d.con_n[c];
-        const double overlap = cn.w;
-        if (!(invSum <= 0.0 || overlap <= 0.0)) {
-            const V3 corr = v3of(cn) * (a.beta * overlap / invSum);
-            if (d.meta[i].y & kFlagMutable) d.pos[i] = d4of(v3of(pa) + corr * pa.w, pa.w);
-            if (d.meta[j].y & kFlagMutable) d.pos[j] = d4of(v3of(pb) - corr * pb.w, pb.w);
-        }
-        if (a.warm) d.wimp[ctl->wsel ^ 1][c] = d.con_imp[c].x;
+        __syncthreads();
     }
 }
 
@@ -820,8 +1056,15 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
     k_island_mark<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a, ib); ++L;
     scan_u32(d.iflag, d.ioff, (uint32_t)a.Ccap, d.tsum, &ctl->scan_total, ctl, st, launches);
     k_island_start<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a); ++L;
+    // Per-body update ranks for the dataflow solver.
+    k_rank_entries<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a, ib); ++L;
+    uint32_t* rks[2] = {d.rkey[0], d.rkey[1]};
+    uint32_t* rvs[2] = {d.rval[0], d.rval[1]};
+    const int rb = radix_sort_u32(rks, rvs, (uint32_t)(2 * a.Ccap), lbits, d.hist, d.tsum, ctl, st, launches);
+    k_rank_write<<<blocks_for(2 * a.Ccap, kT), kT, 0, st>>>(a, rb); ++L;
     mark(6);
     k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib); ++L;
+    k_island_solve_big<<<a.num_sms, kBigThreads, 0, st>>>(a, ib, rb); ++L;
     mark(7);
     k_boundary<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
     k_step_end<<<1, 1, 0, st>>>(a); ++L;

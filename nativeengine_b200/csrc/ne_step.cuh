@@ -22,6 +22,7 @@ struct StepArgs {
     int key_bits;            // bits the cell-key sort covers this step
     // capacities
     uint64_t Pcap, Scap, Ccap;
+    int num_sms;
 };
 
 // ev: NE_NUM_STAGES + 1 events recorded at the stage boundaries, or nullptr.
