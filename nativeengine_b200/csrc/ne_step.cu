@@ -65,6 +65,7 @@ __device__ __forceinline__ long long cell_of(const StepArgs& a, double c, int ax
 struct KeyLayout {
     int bits[3];
     long long base[3];
+    long long span[3];   // occupied offsets are [0, span] per axis
     int total;
 };
 
@@ -75,10 +76,12 @@ __device__ __forceinline__ KeyLayout key_layout(const StepArgs& a, const Ctl* ct
             const long long m = a.nc[ax];
             L.bits[ax] = (m > (1ll << 21)) ? 21 : bitlen_u64((unsigned long long)(m - 1));
             L.base[ax] = 0;
+            L.span[ax] = m - 1;
         } else {
             const long long span = ctl->cmax[ax] - ctl->cmin[ax];
             L.bits[ax] = (span >= (1ll << 21) || span < 0) ? 21 : bitlen_u64((unsigned long long)span);
             L.base[ax] = ctl->cmin[ax];
+            L.span[ax] = span;
         }
     }
     L.total = L.bits[0] + L.bits[1] + L.bits[2];
@@ -94,6 +97,24 @@ __device__ __forceinline__ unsigned long long compact_key(const KeyLayout& L, lo
     return x | (y << L.bits[0]) | (z << (L.bits[0] + L.bits[1]));
 }
 
+// Key of a neighbour cell.  A cell outside the occupied offset range holds no
+// body; with fewer than 21 bits per axis its offset would not fit its field
+// and would alias another cell, so it gets kNoCell, which matches nothing.
+// (With 21 bits every offset fits, and aliasing modulo 2^21 is exactly the
+// reference's masking.)
+constexpr unsigned long long kNoCell = ~0ull;
+
+__device__ __forceinline__ unsigned long long neighbour_key(const KeyLayout& L, long long cx, long long cy,
+                                                            long long cz) {
+    const long long c[3] = {cx, cy, cz};
+    for (int ax = 0; ax < 3; ++ax) {
+        if (L.bits[ax] >= 21) continue;
+        const long long off = c[ax] - L.base[ax];
+        if (off < 0 || off > L.span[ax]) return kNoCell;
+    }
+    return compact_key(L, cx, cy, cz);
+}
+
 __device__ __forceinline__ long long wrap_cell(const StepArgs& a, long long c, int axis) {
     if (!a.dom.periodic) return c;
     const long long m = a.nc[axis];
@@ -107,8 +128,8 @@ __device__ __forceinline__ int neighbour_keys(const StepArgs& a, const KeyLayout
     for (int dx = -1; dx <= 1; ++dx)
         for (int dy = -1; dy <= 1; ++dy)
             for (int dz = -1; dz <= 1; ++dz) {
-                unsigned long long k = compact_key(L, wrap_cell(a, cx + dx, 0), wrap_cell(a, cy + dy, 1),
-                                                   wrap_cell(a, cz + dz, 2));
+                unsigned long long k = neighbour_key(L, wrap_cell(a, cx + dx, 0), wrap_cell(a, cy + dy, 1),
+                                                     wrap_cell(a, cz + dz, 2));
                 bool dup = false;
                 for (int t = 0; t < nk; ++t) dup |= (out[t] == k);
                 if (!dup) out[nk++] = k;
@@ -329,8 +350,8 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
     uint32_t rlo = 0, rhi = 0;
     if (lane < 27) {
         const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
-        unsigned long long k = compact_key(L, wrap_cell(a, cx + dx, 0), wrap_cell(a, cy + dy, 1),
-                                           wrap_cell(a, cz + dz, 2));
+        unsigned long long k = neighbour_key(L, wrap_cell(a, cx + dx, 0), wrap_cell(a, cy + dy, 1),
+                                             wrap_cell(a, cz + dz, 2));
         const uint32_t grp = __match_any_sync(0x07ffffffu, k);
         if (lane == __ffs(grp) - 1) {
             uint32_t lo = lower_bound_u64(keys, 0, a.n, k);
@@ -815,8 +836,17 @@ __global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
     for (uint32_t k = s; k < e; ++k) correct_item(d, ord[k], a.beta, wout);
 }
 
-constexpr uint32_t kRoundLimit = 1u << 26;
+// A warp that sees no update complete for this long gives up and reports
+// (ctl->solve_timeout -> NE_ERR_TIMEOUT).  Legitimate waits are bounded by the
+// island's critical path, well under a millisecond per update.
+constexpr unsigned long long kStallNs = 2000000000ull;
 constexpr uint32_t kEmpty = 0xffffffffu;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 constexpr int kBigThreads = 512;
 
 // Island-local view of one contact's update (phase p, contact position pos).
@@ -916,7 +946,8 @@ __global__ void __launch_bounds__(kBigThreads) k_island_solve_big(StepArgs a, in
 
         cuda::atomic_ref<uint32_t, cuda::thread_scope_block> head(s_head);
         uint32_t h = head.fetch_add(1u, cuda::memory_order_relaxed);
-        uint32_t idle = 0;
+        unsigned long long last_progress = global_ns();
+        uint32_t rounds = 0;
         while (true) {
             const bool live = h < total;
             if (!__any_sync(0xffffffffu, live)) break;
@@ -941,9 +972,17 @@ __global__ void __launch_bounds__(kBigThreads) k_island_solve_big(StepArgs a, in
                 if (sj != kEmpty) big_notify(cnt, queue, &s_tail, sj);
                 h = head.fetch_add(1u, cuda::memory_order_relaxed);
             }
-            idle = __any_sync(0xffffffffu, ready) ? 0u : idle + 1u;
+            // Check the clock every 64 idle rounds; lane 0's reading decides
+            // for the warp so the exit is warp-uniform.
+            bool stalled = false;
+            if (__any_sync(0xffffffffu, ready)) {
+                rounds = 0;
+                last_progress = global_ns();
+            } else if ((++rounds & 63u) == 0u) {
+                stalled = __shfl_sync(0xffffffffu, global_ns() - last_progress > kStallNs ? 1 : 0, 0) != 0;
+            }
             const bool failed = __any_sync(0xffffffffu, *(volatile int*)&s_fail != 0);   // warp-uniform
-            if (idle > kRoundLimit || failed) {
+            if (stalled || failed) {
                 if ((threadIdx.x & 31) == 0) {
                     s_fail = 1;
                     atomicExch(&ctl->solve_timeout, 1u);
