@@ -226,6 +226,27 @@ int ne_world_profile(NeWorld* world, int enable);
 int ne_world_stage_times(NeWorld* world, double* ms, uint64_t* steps);
 const char* ne_stage_name(int stage);
 
+/* Broadphase pair list without any device allocation.  No counterpart in the
+ * reference: it is for callers that may not allocate GPU memory where they
+ * call -- an embedding engine that hands out device memory only from its own
+ * fixed pool, or a frame loop in which an allocation (and the synchronisation
+ * cudaMalloc/cudaFree can bring) is not allowed.  Returns, for the bodies as
+ * given, the sorted unique candidate pairs World::broadphasePairs() would
+ * return (the same list ne_world_pairs reports for a step); at most cap pairs
+ * are written to the host arrays and *count receives the total.  All device
+ * working memory is one file-scope array (about 2.1 MiB) that every GPU the
+ * library is loaded on holds until the process exits; more than
+ * NE_NOALLOC_MAX_BODIES bodies or NE_NOALLOC_MAX_PAIRS pairs is refused with
+ * NE_ERR_CAPACITY.  Every call shares that array, so calls that overlap on the
+ * GPU (several host threads at once) race and must be serialised by the
+ * caller.  The first call on a device looks up the array's device address;
+ * make it before any stream capture.  Synchronous, on the per-thread default
+ * stream. */
+#define NE_NOALLOC_MAX_BODIES 2048u
+#define NE_NOALLOC_MAX_PAIRS 262144u
+int ne_broadphase_pairs_noalloc(const NeWorldParams* params, const NeBodyArrays* bodies, uint32_t* pair_i,
+                                uint32_t* pair_j, uint64_t cap, uint64_t* count);
+
 /* Human-readable status / last CUDA error text. */
 const char* ne_status_string(int status);
 const char* ne_last_error(void);

@@ -23,6 +23,8 @@ NE_ERR_TIMEOUT = 5
 NE_ERR_NUMERIC = 6
 NE_ERR_NO_DEVICE = 7
 NUM_STAGES = 8
+NOALLOC_MAX_BODIES = 2048
+NOALLOC_MAX_PAIRS = 262144
 
 # shapes (ne::Shape order)
 SPHERE, CYLINDER, BOX, CAPSULE, CONVEX, PLANE, MESH, COMPOUND = range(8)
@@ -111,6 +113,8 @@ EXPORTS = {
     "ne_world_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "ne_world_stage_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "ne_stage_name": (C.c_char_p, [C.c_int]),
+    "ne_broadphase_pairs_noalloc": (C.c_int, [C.POINTER(NeWorldParams), C.POINTER(NeBodyArrays), C.c_void_p,
+                                              C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     "ne_status_string": (C.c_char_p, [C.c_int]),
     "ne_last_error": (C.c_char_p, []),
 }

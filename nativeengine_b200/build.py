@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib", "libne_cuda.so")
-SOURCES = ["ne_prims.cu", "ne_step.cu", "ne_capi.cu"]
+SOURCES = ["ne_prims.cu", "ne_step.cu", "ne_capi.cu", "ne_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 

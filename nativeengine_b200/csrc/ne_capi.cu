@@ -52,6 +52,11 @@ inline size_t grow_to(uint64_t need) { return (size_t)(need + need / 4 + 1024); 
 
 }  // namespace
 
+namespace neb {
+// Lets other translation units of the library report through ne_last_error().
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace neb
+
 struct NeWorld {
     NeWorldParams p{};
     int device = 0;
