@@ -42,6 +42,29 @@ WORKLOAD = ("box_pile_4096: static ground box (50,1,50) + 4,096 boxes, half exte
             "density 1, random unit quaternions, 16^3 lattice spacing 1.6 from y=2; open boundary, "
             "mu=0.5, e=0.2, g=-9.81, dt=1/60, from the initial state (seed 2)")
 L2_FLUSH_BYTES = 256 << 20
+
+
+def _cfg_box_pile():
+    from nativeengine_b200 import scenes
+    return scenes.box_pile()
+
+
+def _cfg_box_pile_8():
+    from nativeengine_b200 import scenes
+    return scenes.box_pile(8, 8, 8)
+
+
+def _cfg_gas():
+    from nativeengine_b200 import scenes
+    return scenes.gas()
+
+
+CONFIGS = {
+    "box_pile": (_cfg_box_pile, WORKLOAD),
+    "box_pile_8": (_cfg_box_pile_8, "box_pile_512: as box_pile_4096 on an 8^3 lattice (profiling case)"),
+    "gas": (_cfg_gas, "gas_1000: periodic elastic gas, 1,000 spheres r=0.5 m=1, L=25, v~N(0,1), e=1, mu=0, "
+                      "g=0, dt=1/60 (seed 1)"),
+}
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "solve_box_pile_4096.md")
 
 
@@ -52,6 +75,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="box_pile",
+                    help="workload (box_pile is the headline; the others are for profiling and extra lines)")
     return ap.parse_args()
 
 
@@ -210,9 +235,10 @@ def run_ours(args):
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    from nativeengine_b200 import DeviceWorld, scenes
+    from nativeengine_b200 import DeviceWorld
 
-    params, bodies = scenes.box_pile()
+    make, workload = CONFIGS[args.config]
+    params, bodies = make()
     n = bodies.n
     dev = DeviceWorld(params, bodies.copy())
     stream = torch.cuda.ExternalStream(dev.stream_handle())
@@ -293,7 +319,7 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
             "ms_per_step": t_dev / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "bodies": n, "steps_per_run": K,
+            "config": {"workload": workload, "bodies": n, "steps_per_run": K,
                        "parallelism": "replicas" if world > 1 else "single world",
                        "l2": "256 MiB buffer rewritten between timed steps (outside the events)"},
             "roofline": {"bound": "hbm", "kernel": "solve (k_island_solve + k_island_solve_big)",
@@ -312,7 +338,7 @@ def run_ours(args):
             "step_roofline": {"algorithmic_bytes_last_step": step_bytes,
                               "achieved_gbs_mean": step_bytes / (t_dev / K) / 1e9},
         }
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and args.config == "box_pile":
             line["cpu_baseline"] = cpu_baseline_reference()
         print(json.dumps(line))
     dev.close()
