@@ -65,7 +65,7 @@ CONFIGS = {
     "gas": (_cfg_gas, "gas_1000: periodic elastic gas, 1,000 spheres r=0.5 m=1, L=25, v~N(0,1), e=1, mu=0, "
                       "g=0, dt=1/60 (seed 1)"),
 }
-PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "solve_box_pile_4096.md")
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "solve_box_pile_512.md")
 
 
 def parse_args():
@@ -93,16 +93,17 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
-    summary (a line 'traffic_bytes_per_launch: N'), else None."""
+def profile_traffic(contacts):
+    """DRAM bytes of one solver launch: the per-contact traffic of the
+    committed ncu capture (a smaller pile; line 'traffic_bytes_per_contact: N')
+    scaled by the contacts of the measured step, else None."""
     if not os.path.exists(PROFILE_SUMMARY):
         return None
     with open(PROFILE_SUMMARY) as f:
         for line in f:
-            if line.strip().startswith("traffic_bytes_per_launch:"):
+            if line.strip().startswith("traffic_bytes_per_contact:"):
                 try:
-                    return float(line.split(":", 1)[1].strip().split()[0])
+                    return float(line.split(":", 1)[1].strip().split()[0]) * contacts
                 except ValueError:
                     return None
     return None
@@ -324,7 +325,7 @@ def run_ours(args):
                        "l2": "256 MiB buffer rewritten between timed steps (outside the events)"},
             "roofline": {"bound": "hbm", "kernel": "solve (k_island_solve + k_island_solve_big)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": peak_kind, "traffic": profile_traffic(),
+                         "peak_source": peak_kind, "traffic": profile_traffic(C_last),
                          "note": "latency-bound: the exact Gauss-Seidel order is a dependency chain; "
                                  "algorithmic bytes = 144 B/contact + 200 B/body of the last step"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * 32 * n,
