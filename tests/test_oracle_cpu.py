@@ -65,3 +65,42 @@ def test_factories_match_reference(kind, p, verts):
         got = B.convex_mass(verts, 1.3)
     want = O.ref_mass_props(kind, p, verts, 1.3)
     assert got[0] == want[0] and tuple(got[1]) == tuple(want[1])
+
+
+needs_port = pytest.mark.skipif(not O.port_available(), reason="oracle/_build/libne_oracle.so not built")
+
+
+@needs_port
+@pytest.mark.parametrize("name", golden_io.names())
+def test_port_reproduces_golden(name):
+    """The C restatement (oracle/ne_oracle.c) gives the reference's bits."""
+    params, bodies, expected = golden_io.load(name)
+    port = O.PortOracle(params, bodies)
+    for s, e in enumerate(expected):
+        port.step(1)
+        assert np.array_equal(port.pairs(), e["pairs"]), f"{name} step {s}: pairs"
+        c = port.contacts()
+        for k in ("i", "j", "slot", "point", "normal", "depth", "n_imp"):
+            assert np.array_equal(c[k], e["c_" + k]), f"{name} step {s}: contact {k}"
+        assert np.array_equal(port.islands(), e["islands"])
+        st = port.state()
+        for k in ("x", "q", "v", "w"):
+            assert np.array_equal(st[k], e[k]), f"{name} step {s}: {k}"
+
+
+@needs_ref
+@needs_port
+@pytest.mark.parametrize("make,steps", [
+    (lambda: __import__("nativeengine_b200.scenes", fromlist=["x"]).box_pile(6, 6, 6), 60),
+    (lambda: __import__("nativeengine_b200.scenes", fromlist=["x"]).gas(n=400, half=8.0), 60),
+    (lambda: __import__("nativeengine_b200.scenes", fromlist=["x"]).mixed_shapes(n=150, seed=99), 40),
+])
+def test_port_matches_reference_trajectory(make, steps):
+    params, bodies = make()
+    ref = O.RefOracle(params, bodies.copy())
+    port = O.PortOracle(params, bodies.copy())
+    ref.step(steps)
+    port.step(steps)
+    a, b = ref.state(), port.state()
+    for k in ("x", "q", "v", "w"):
+        assert np.array_equal(a[k], b[k]), k
