@@ -59,12 +59,23 @@ def _cfg_gas():
     return scenes.gas()
 
 
+def _cfg_granular():
+    from nativeengine_b200 import scenes
+    return scenes.granular_mix(n=65536, max_attempts=2000)
+
+
 CONFIGS = {
     "box_pile": (_cfg_box_pile, WORKLOAD),
     "box_pile_8": (_cfg_box_pile_8, "box_pile_512: as box_pile_4096 on an 8^3 lattice (profiling case)"),
     "gas": (_cfg_gas, "gas_1000: periodic elastic gas, 1,000 spheres r=0.5 m=1, L=25, v~N(0,1), e=1, mu=0, "
                       "g=0, dt=1/60 (seed 1)"),
+    "granular": (_cfg_granular, "granular_65536: periodic mix of spheres/capsules/cylinders/12-point hulls "
+                                "(types by index mod 4), exact-overlap random sequential placement at the "
+                                "densest box that places all bodies (true-volume packing fraction ~0.19), "
+                                "v~N(0,0.5), mu=0.3, e=0.5, g=0, dt=1/60 (seed 3)"),
 }
+# Reference-CPU sample per config: physics steps timed on one host core.
+CPU_SAMPLE_STEPS = {"box_pile": 3, "box_pile_8": 20, "gas": 2000, "granular": 2}
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "solve_box_pile_512.md")
 
 
@@ -159,20 +170,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sms)}
 
 
-def cpu_baseline_reference(steps: int = 3):
+def cpu_baseline_reference(config: str, params, bodies):
     """The reference step (oracle/_ref, one host core) on a bounded sample:
-    the first `steps` steps of the same workload."""
-    from nativeengine_b200 import scenes
+    the first few steps of the same workload."""
     from oracle import oracle as O
     if not O.ref_available():
         return None
-    params, bodies = scenes.box_pile()
-    ora = O.RefOracle(params, bodies)
+    steps = CPU_SAMPLE_STEPS[config]
+    ora = O.RefOracle(params, bodies.copy())
     t0 = time.perf_counter()
     ora.step_plain(steps)
     dt = time.perf_counter() - t0
     return {"value": bodies.n * steps / dt, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"first {steps} steps of box_pile_4096 on one host core ({dt:.1f} s)"}
+            "sample": f"first {steps} steps of {config} ({bodies.n} bodies) on one host core ({dt:.1f} s)"}
 
 
 def _ref_worker(args):
@@ -339,8 +349,8 @@ def run_ours(args):
             "step_roofline": {"algorithmic_bytes_last_step": step_bytes,
                               "achieved_gbs_mean": step_bytes / (t_dev / K) / 1e9},
         }
-        if world == 1 and not args.no_cpu_baseline and args.config == "box_pile":
-            line["cpu_baseline"] = cpu_baseline_reference()
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline_reference(args.config, params, bodies)
         print(json.dumps(line))
     dev.close()
     if world > 1:

@@ -33,6 +33,27 @@ def _stale(out, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+HOST_SRC = os.path.join(HERE, "host", "src", "world.cpp")
+HOST_SCENES = os.path.join(HERE, "host", "src", "scenes.cpp")
+HOST_INC = os.path.join(HERE, "host", "include")
+HOST_OUT = os.path.join(HERE, "_lib", "libne_host.so")
+
+
+def build_host(force: bool = False, verbose: bool = False) -> str:
+    """The C++17 facade (ne::World / ne::PhysicsWorld) over libne_cuda.so."""
+    deps = [HOST_SRC, HOST_SCENES, OUT, os.path.join(HOST_INC, "ne", "world.hpp"),
+            os.path.join(HOST_INC, "ne", "vmath.hpp"), os.path.join(CSRC, "ne_geom.cuh")]
+    if force or _stale(HOST_OUT, deps):
+        cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-fPIC", "-shared", "-I" + HOST_INC,
+               "-I" + os.path.join(ROOT, "include"), "-I" + CSRC, HOST_SRC, HOST_SCENES,
+               "-L" + os.path.dirname(OUT), "-lne_cuda",
+               "-Wl,-rpath,$ORIGIN", "-o", HOST_OUT]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    return HOST_OUT
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "ne_cuda.h")]
     if force or _stale(OUT, deps):
@@ -42,6 +63,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+    build_host(force=force, verbose=verbose)
     return OUT
 
 

@@ -16,6 +16,9 @@
 #define NE_HD __host__ __device__ __forceinline__
 #else
 #define NE_HD inline
+#ifndef __align__
+#define __align__(n) __attribute__((aligned(n)))
+#endif
 #endif
 
 namespace neb {

@@ -89,66 +89,74 @@ def _hull_points(rng, npts=12, scale=0.5):
     return pts
 
 
-def granular_mix(n: int = 65536, phi: float = 0.3, seed: int = 3, max_attempts: int = 60,
-                 dt: float = 1.0 / 60.0):
-    """Periodic granular mix, placed by random sequential addition with
-    bounding-sphere rejection.  The box edge is chosen for the target packing
-    fraction of the true shape volumes and grown until every body places."""
+def granular_mix(n: int = 65536, phi: float = 0.3, seed: int = 3, max_attempts: int = 400,
+                 dt: float = 1.0 / 60.0, grow: float = 1.02):
+    """Periodic granular mix (types by index mod 4: sphere r U[0.3,0.6], capsule
+    r 0.25 half-height U[0.2,0.6], cylinder r 0.3 height 0.8, convex hull of 12
+    points uniform in the unit ball scaled by 0.5), random orientations,
+    v ~ N(0, 0.5) per axis, mu 0.3, e 0.5, g 0.  Bodies are placed by random
+    sequential addition with exact (GJK) overlap rejection; the box edge starts
+    at the target packing fraction of the true shape volumes and grows by
+    `grow` until every body places.  The achieved fraction is stored as
+    ``packing_fraction`` on the returned BodyArrays."""
+    import ctypes as C
     rng = _rng(seed)
-    protos = []
+    bodies: List[Body] = []
     vols = []
     for idx in range(n):
         t = idx % 4
+        q = random_quat(rng)
         if t == 0:
             r = rng.uniform(0.3, 0.6)
-            protos.append(("s", r))
+            b = make_sphere((0.0, 0.0, 0.0), r, 1.0)
             vols.append(4.0 / 3.0 * math.pi * r ** 3)
         elif t == 1:
             hh = rng.uniform(0.2, 0.6)
-            protos.append(("c", 0.25, hh))
+            b = make_capsule((0.0, 0.0, 0.0), q, 0.25, hh, 1.0)
             vols.append(math.pi * 0.25 ** 2 * 2 * hh + 4.0 / 3.0 * math.pi * 0.25 ** 3)
         elif t == 2:
-            protos.append(("y", 0.3, 0.8))
+            b = make_cylinder((0.0, 0.0, 0.0), q, 0.3, 0.8, 1.0)
             vols.append(math.pi * 0.09 * 0.8)
         else:
             pts = _hull_points(rng)
-            protos.append(("h", pts))
+            b = make_convex((0.0, 0.0, 0.0), q, pts, 1.0)
             vols.append(_hull_volume(np.array(pts)))
-    bound = []
-    for p in protos:
-        if p[0] == "s":
-            bound.append(p[1])
-        elif p[0] == "c":
-            bound.append(p[1] + p[2])
-        elif p[0] == "y":
-            bound.append(math.sqrt(0.4 * 0.4 + 0.3 * 0.3))
-        else:
-            bound.append(max(math.sqrt(x * x + y * y + z * z) for x, y, z in p[1]))
-    bound = np.array(bound)
-    L = (sum(vols) / phi) ** (1.0 / 3.0)
-    while True:
-        centres = _rsa_periodic(bound, L, rng, max_attempts)
-        if centres is not None:
-            break
-        L *= 1.03
-    half = L / 2.0
-    bodies: List[Body] = []
-    for idx, (p, c) in enumerate(zip(protos, centres)):
-        q = random_quat(rng)
-        if p[0] == "s":
-            b = make_sphere(tuple(c), p[1], 1.0)
-        elif p[0] == "c":
-            b = make_capsule(tuple(c), q, p[1], p[2], 1.0)
-        elif p[0] == "y":
-            b = make_cylinder(tuple(c), q, p[1], p[2], 1.0)
-        else:
-            b = make_convex(tuple(c), q, p[1], 1.0)
         b.v = tuple(rng.normal(0.0, 0.5, 3))
         bodies.append(b)
-    params = default_params(half=half, periodic=1, dt=dt, friction=0.3, restitution=0.5, gravity=(0, 0, 0))
     ba = BodyArrays(bodies)
+    lib = _host_lib()
+    L = (sum(vols) / phi) ** (1.0 / 3.0)
+    xs = np.zeros((n, 3))
+    dp = lambda a: a.ctypes.data_as(C.c_void_p)
+    while True:
+        placed = lib.ne_scene_place_periodic(n, dp(ba.shape), dp(ba.radius), dp(ba.half_height), dp(ba.half_extents),
+                                             dp(ba.q), dp(ba.vert_offset), dp(ba.vert_count), dp(ba.verts), L,
+                                             seed, max_attempts, dp(xs))
+        if placed == n:
+            break
+        L *= grow
+    ba.x[:] = xs
+    params = default_params(half=L / 2.0, periodic=1, dt=dt, friction=0.3, restitution=0.5, gravity=(0, 0, 0))
     ba.packing_fraction = float(sum(vols) / L ** 3)
     return params, ba
+
+
+_HOST = None
+
+
+def _host_lib():
+    """libne_host.so (scene placement lives there; it is host code)."""
+    global _HOST
+    if _HOST is None:
+        import ctypes as C
+        import os
+        path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libne_host.so")
+        lib = C.CDLL(path)
+        fn = lib.ne_scene_place_periodic
+        fn.restype = C.c_uint32
+        fn.argtypes = [C.c_uint32] + [C.c_void_p] * 8 + [C.c_double, C.c_uint64, C.c_uint32, C.c_void_p]
+        _HOST = lib
+    return _HOST
 
 
 def _hull_volume(pts: np.ndarray) -> float:
@@ -158,48 +166,6 @@ def _hull_volume(pts: np.ndarray) -> float:
     except Exception:
         ext = pts.max(0) - pts.min(0)
         return float(np.prod(ext)) * 0.3
-
-
-def _rsa_periodic(bound: np.ndarray, L: float, rng, max_attempts: int):
-    """Sequential placement with a cell list; None if some body never fits."""
-    n = len(bound)
-    cell = 2.0 * float(bound.max())
-    nc = max(1, int(math.floor(L / cell)))
-    cs = L / nc
-    grid = {}
-    centres = np.empty((n, 3))
-    for i in range(n):
-        ri = bound[i]
-        ok = False
-        for _ in range(max_attempts):
-            c = rng.uniform(-L / 2, L / 2, 3)
-            g = tuple(int(math.floor((c[a] + L / 2) / cs)) % nc for a in range(3))
-            clash = False
-            for dx in (-1, 0, 1):
-                for dy in (-1, 0, 1):
-                    for dz in (-1, 0, 1):
-                        key = ((g[0] + dx) % nc, (g[1] + dy) % nc, (g[2] + dz) % nc)
-                        for j in grid.get(key, ()):
-                            d = centres[j] - c
-                            d -= L * np.floor(d / L + 0.5)
-                            rr = ri + bound[j]
-                            if d @ d < rr * rr:
-                                clash = True
-                                break
-                        if clash:
-                            break
-                    if clash:
-                        break
-                if clash:
-                    break
-            if not clash:
-                ok = True
-                break
-        if not ok:
-            return None
-        centres[i] = c
-        grid.setdefault(g, []).append(i)
-    return centres
 
 
 # ---- small worlds for parity tests -----------------------------------------
