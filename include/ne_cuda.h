@@ -177,6 +177,15 @@ int ne_world_set_params(NeWorld* world, const NeWorldParams* params);
  * (src/physics_world.hpp:58-165,262-270) end here.  Does not clear the warm
  * cache, matching the reference, whose cache survives body edits. */
 int ne_world_upload(NeWorld* world, const NeBodyArrays* bodies);
+/* Batch of independent worlds stepped together (no counterpart in the
+ * reference, which steps one World at a time).  World k owns bodies
+ * [world_begin[k], world_begin[k+1]) of `bodies` (world_begin has nworlds + 1
+ * entries, from 0 to bodies->n) and is configured by params[k]; no pair,
+ * contact or island spans two worlds, so each world evolves exactly as an
+ * ne::World of its own would.  All worlds share one warm_start setting.
+ * Pairs, contacts and island labels of a batch use global body indices. */
+int ne_world_upload_batch(NeWorld* world, const NeWorldParams* params, uint32_t nworlds,
+                          const uint32_t* world_begin, const NeBodyArrays* bodies);
 /* Overwrite only x/q/v/w (each may be NULL to keep the device copy).  Same
  * count as the last full upload. */
 int ne_world_upload_state(NeWorld* world, const double* x, const double* q,

@@ -100,6 +100,8 @@ EXPORTS = {
     "ne_world_destroy": (C.c_int, [C.c_void_p]),
     "ne_world_set_params": (C.c_int, [C.c_void_p, C.POINTER(NeWorldParams)]),
     "ne_world_upload": (C.c_int, [C.c_void_p, C.POINTER(NeBodyArrays)]),
+    "ne_world_upload_batch": (C.c_int, [C.c_void_p, C.POINTER(NeWorldParams), C.c_uint32, C.c_void_p,
+                                        C.POINTER(NeBodyArrays)]),
     "ne_world_upload_state": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ne_world_download": (C.c_int, [C.c_void_p, C.POINTER(NeBodyArrays)]),
     "ne_world_step": (C.c_int, [C.c_void_p, C.c_uint32]),

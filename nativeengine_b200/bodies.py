@@ -296,3 +296,37 @@ def params_dict(p: _ffi.NeWorldParams) -> dict:
     d = {name: getattr(p, name) for name, _ in p._fields_}
     d["gravity"] = tuple(p.gravity)
     return d
+
+
+def concat(parts):
+    """Concatenate BodyArrays into one batch; returns (BodyArrays, world_begin).
+    Convex vertex offsets and noCollide indices are rebased onto the batch."""
+    out = BodyArrays.__new__(BodyArrays)
+    begin = [0]
+    for b in parts:
+        begin.append(begin[-1] + b.n)
+    out.n = begin[-1]
+    per_body = ("x", "q", "v", "w", "force", "torque", "inv_mass", "inv_inertia", "shape", "radius",
+                "half_height", "half_extents", "friction", "restitution", "linear_damping", "angular_damping",
+                "gravity_scale", "layer", "mask", "flags", "vert_count", "nocollide_count")
+    for k in per_body:
+        setattr(out, k, np.ascontiguousarray(np.concatenate([getattr(b, k) for b in parts])))
+    vo, nco, verts, ncl = [], [], [], []
+    vbase = nbase = 0
+    for b, b0 in zip(parts, begin):
+        vo.append(b.vert_offset.astype(np.int64) + vbase)
+        verts.append(b.verts[: b.n_verts])
+        vbase += b.n_verts
+        nco.append(b.nocollide_offset.astype(np.int64) + nbase)
+        ncl.append(b.nocollide[: b.n_nocollide].astype(np.int64) + b0)
+        nbase += b.n_nocollide
+    out.vert_offset = np.concatenate(vo).astype(np.uint32)
+    out.n_verts = vbase
+    v = np.concatenate(verts) if vbase else np.zeros((1, 3))
+    out.verts = np.ascontiguousarray(v.reshape(-1, 3), dtype=np.float64)
+    out.nocollide_offset = np.concatenate(nco).astype(np.uint32)
+    out.n_nocollide = nbase
+    nc = np.concatenate(ncl) if nbase else np.zeros(1)
+    out.nocollide = np.ascontiguousarray(nc, dtype=np.uint32)
+    out._c = None
+    return out, np.array(begin, dtype=np.uint32)

@@ -64,11 +64,18 @@ struct NeWorld {
     uint32_t n = 0;
     neb::DevWorld d{};
     neb::Ctl* h_ctl = nullptr;   // pinned mirror of d.ctl
-    // broadphase constants
-    double max_r = 0.0, cell = 0.0;
-    long long nc[3] = {1, 1, 1};
-    int brute = 1;
-    uint32_t nplanes = 0;
+    // worlds of the batch (a single ne::World is a batch of one)
+    uint32_t nworlds = 1;
+    std::vector<NeWorldParams> wparams;   // [nworlds]
+    std::vector<uint32_t> wbegin;         // [nworlds + 1] body ranges
+    std::vector<double> h_bound;          // bounding radius per body (grid constants)
+    std::vector<int> h_shape;
+    std::vector<neb::WorldP> h_wp;
+    neb::WorldP* d_wp = nullptr;
+    uint32_t* d_bw = nullptr;             // world of each body
+    long long* d_cext = nullptr;          // per-world cell extents
+    int world_bits = 0;
+    int any_grid = 0;
     int key_bits = 64;
     int num_sms = 148;
     // capacities (entries)
@@ -198,22 +205,14 @@ neb::StepArgs make_args(const NeWorld* w) {
     neb::StepArgs a;
     a.d = w->d;
     a.n = w->n;
-    a.dom.half = w->p.half;
-    a.dom.periodic = w->p.periodic ? 1 : 0;
-    a.dt = w->p.dt;
-    a.restitution = w->p.restitution;
-    a.friction = w->p.friction;
-    a.beta = w->p.contact_beta;
-    a.g = neb::mk(w->p.gravity[0], w->p.gravity[1], w->p.gravity[2]);
-    a.rcomb = w->p.restitution_combine;
-    a.fcomb = w->p.friction_combine;
-    a.warm = w->p.warm_start ? 1 : 0;
-    a.open_boundary = w->p.open_boundary ? 1 : 0;
-    a.cell = w->cell;
-    for (int k = 0; k < 3; ++k) a.nc[k] = w->nc[k];
-    a.brute = w->brute;
-    a.nplanes = w->nplanes;
+    a.nworlds = w->nworlds;
+    a.world_bits = w->world_bits;
+    a.wp = w->d_wp;
+    a.bw = w->d_bw;
+    a.cext = w->d_cext;
     a.key_bits = w->key_bits;
+    a.any_grid = w->any_grid;
+    a.warm = w->wparams.empty() ? (w->p.warm_start ? 1 : 0) : (w->wparams[0].warm_start ? 1 : 0);
     a.Pcap = w->Pcap;
     a.Scap = w->Scap;
     a.Ccap = w->Ccap;
@@ -230,40 +229,78 @@ int check_params(const NeWorldParams* p) {
     return NE_OK;
 }
 
-// Broadphase constants of World::broadphasePairs() (src/world.cpp:427-457):
-// cell = 2 * max bounding radius over grid bodies, brute force below 64
-// bodies, periodic cell counts nc = max(1, floor(L / cell)).
-void derive_grid(NeWorld* w, const std::vector<double>& boundR, const std::vector<int>& shape) {
-    double maxR = 0.0;
-    w->nplanes = 0;
-    for (uint32_t i = 0; i < w->n; ++i) {
-        if (shape[i] == NE_SHAPE_PLANE || shape[i] == NE_SHAPE_MESH) { ++w->nplanes; continue; }
-        maxR = (maxR < boundR[i]) ? boundR[i] : maxR;
-    }
-    w->max_r = maxR;
-    w->cell = 2.0 * maxR;
-    w->brute = (w->p.force_brute_force || w->n < 64 || w->cell < 1e-9) ? 1 : 0;
-    w->nc[0] = w->nc[1] = w->nc[2] = 1;
-    if (w->p.periodic && !w->brute) {
-        const double L = 2.0 * w->p.half;
-        for (int a = 0; a < 3; ++a) {
-            long long m = (long long)(int)std::floor(L / w->cell);
-            w->nc[a] = m < 1 ? 1 : m;
+// Per-world constants of World::broadphasePairs() (src/world.cpp:427-457):
+// cell = 2 * max bounding radius over the world's grid bodies, brute force
+// below 64 bodies, periodic cell counts nc = max(1, floor(L / cell)); the
+// range of the world's planes in the (ascending) plane list; and the bits the
+// cell-key sort needs when every grid world is periodic.
+int derive_worlds(NeWorld* w, const std::vector<uint32_t>& planes) {
+    const uint32_t nw = w->nworlds;
+    w->h_wp.assign(nw, neb::WorldP{});
+    w->any_grid = 0;
+    int local_bits = 0;
+    bool all_periodic = true;
+    size_t pk = 0;
+    for (uint32_t k = 0; k < nw; ++k) {
+        const NeWorldParams& p = w->wparams[k];
+        neb::WorldP& W = w->h_wp[k];
+        W.dom.half = p.half;
+        W.dom.periodic = p.periodic ? 1 : 0;
+        W.dt = p.dt;
+        W.restitution = p.restitution;
+        W.friction = p.friction;
+        W.beta = p.contact_beta;
+        W.g = neb::mk(p.gravity[0], p.gravity[1], p.gravity[2]);
+        W.rcomb = p.restitution_combine;
+        W.fcomb = p.friction_combine;
+        W.open_boundary = p.open_boundary ? 1 : 0;
+        W.begin = w->wbegin[k];
+        W.end = w->wbegin[k + 1];
+        double maxR = 0.0;
+        for (uint32_t i = W.begin; i < W.end; ++i) {
+            if (w->h_shape[i] == NE_SHAPE_PLANE || w->h_shape[i] == NE_SHAPE_MESH) continue;
+            maxR = (maxR < w->h_bound[i]) ? w->h_bound[i] : maxR;
+        }
+        W.cell = 2.0 * maxR;
+        W.brute = (p.force_brute_force || (W.end - W.begin) < 64 || W.cell < 1e-9) ? 1 : 0;
+        W.nc[0] = W.nc[1] = W.nc[2] = 1;
+        if (p.periodic && !W.brute) {
+            const double L = 2.0 * p.half;
+            for (int a = 0; a < 3; ++a) {
+                long long m = (long long)(int)std::floor(L / W.cell);
+                W.nc[a] = m < 1 ? 1 : m;
+            }
+        }
+        while (pk < planes.size() && planes[pk] < W.begin) ++pk;
+        W.plane_begin = (uint32_t)pk;
+        while (pk < planes.size() && planes[pk] < W.end) ++pk;
+        W.plane_end = (uint32_t)pk;
+        if (!W.brute) {
+            w->any_grid = 1;
+            if (!p.periodic) all_periodic = false;
+            int bits = 0;
+            for (int a = 0; a < 3; ++a) {
+                long long m = W.nc[a];
+                int b = 0;
+                if (m > (1ll << 21)) b = 21;
+                else while ((1ll << b) < m) ++b;
+                bits += b;
+            }
+            local_bits = std::max(local_bits, bits);
         }
     }
-    if (w->p.periodic) {
-        int bits = 0;
-        for (int a = 0; a < 3; ++a) {
-            long long m = w->nc[a];
-            int b = 0;
-            if (m > (1ll << 21)) b = 21;
-            else while ((1ll << b) < m) ++b;
-            bits += b;
-        }
-        w->key_bits = ((bits + 1 + 7) / 8) * 8;
-    } else {
-        w->key_bits = 64;
-    }
+    w->world_bits = 0;
+    while ((1u << w->world_bits) < nw) ++w->world_bits;
+    w->key_bits = all_periodic ? ((w->world_bits + local_bits + 1 + 7) / 8) * 8 : 64;
+    if (w->key_bits > 64) return set_err(NE_ERR_CAPACITY, "cell keys of this batch need more than 64 bits");
+    neb::DevWorld& d = w->d;
+    (void)d;
+    dfree(w->d_wp);
+    dfree(w->d_cext);
+    int rc;
+    if ((rc = dalloc(&w->d_wp, nw)) || (rc = dalloc(&w->d_cext, 6 * (size_t)nw))) return rc;
+    NE_CUDA_TRY(cudaMemcpy(w->d_wp, w->h_wp.data(), nw * sizeof(neb::WorldP), cudaMemcpyHostToDevice));
+    return NE_OK;
 }
 
 }  // namespace
@@ -339,6 +376,7 @@ int ne_world_destroy(NeWorld* w) {
     dfree(d.verts); dfree(d.nc); dfree(d.planes);
     for (int b = 0; b < 2; ++b) { dfree(d.wkey[b]); dfree(d.wimp[b]); }
     dfree(d.hist); dfree(d.tsum); dfree(d.ctl);
+    dfree(w->d_wp); dfree(w->d_bw); dfree(w->d_cext);
     if (w->h_ctl) cudaFreeHost(w->h_ctl);
     if (w->pinned) cudaFreeHost(w->pinned);
     for (int k = 0; k <= NE_NUM_STAGES; ++k)
@@ -352,27 +390,34 @@ int ne_world_set_params(NeWorld* w, const NeWorldParams* params) {
     if (!w) return set_err(NE_ERR_ARG, "world is NULL");
     int rc = check_params(params);
     if (rc) return rc;
-    const bool regrid = params->half != w->p.half || params->periodic != w->p.periodic ||
-                        params->force_brute_force != w->p.force_brute_force;
+    if (w->nworlds > 1) return set_err(NE_ERR_ARG, "a batch takes its parameters from ne_world_upload_batch");
     w->p = *params;
-    if (regrid && w->has_bodies) {
-        // Recompute the grid constants from the device copy of the shapes.
-        std::vector<neb::D4> inert(w->n);
-        std::vector<uint4> meta(w->n);
-        NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
-        NE_CUDA_TRY(cudaMemcpy(inert.data(), w->d.inert, w->n * sizeof(neb::D4), cudaMemcpyDeviceToHost));
-        NE_CUDA_TRY(cudaMemcpy(meta.data(), w->d.meta, w->n * sizeof(uint4), cudaMemcpyDeviceToHost));
-        std::vector<double> r(w->n);
-        std::vector<int> s(w->n);
-        for (uint32_t i = 0; i < w->n; ++i) { r[i] = inert[i].w; s[i] = (int)meta[i].x; }
-        derive_grid(w, r, s);
+    if (w->has_bodies) {
+        w->wparams.assign(1, *params);
+        std::vector<uint32_t> planes;
+        for (uint32_t i = 0; i < w->n; ++i)
+            if (w->h_shape[i] == NE_SHAPE_PLANE || w->h_shape[i] == NE_SHAPE_MESH) planes.push_back(i);
+        if ((rc = derive_worlds(w, planes))) return rc;
     }
     return NE_OK;
 }
 
-int ne_world_upload(NeWorld* w, const NeBodyArrays* b) {
-    if (!w || !b) return set_err(NE_ERR_ARG, "NULL argument");
+}  // extern "C"
+
+namespace {
+
+int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const uint32_t* wbegin,
+                const NeBodyArrays* b) {
     const uint32_t n = b->n;
+    if (nworlds == 0) return set_err(NE_ERR_ARG, "a batch needs at least one world");
+    if (wbegin[0] != 0 || wbegin[nworlds] != n) return set_err(NE_ERR_ARG, "world ranges must cover [0, n)");
+    for (uint32_t k = 0; k < nworlds; ++k) {
+        if (wbegin[k + 1] < wbegin[k]) return set_err(NE_ERR_ARG, "world ranges must be ascending");
+        int rc = check_params(&params[k]);
+        if (rc) return rc;
+        if ((params[k].warm_start != 0) != (params[0].warm_start != 0))
+            return set_err(NE_ERR_ARG, "all worlds of a batch share one warm_start setting");
+    }
     if (n > (1u << 24)) return set_err(NE_ERR_CAPACITY, "more than 2^24 bodies");
     if (n && (!b->x || !b->q || !b->v || !b->w || !b->inv_mass || !b->inv_inertia || !b->shape || !b->radius ||
               !b->half_height || !b->half_extents || !b->friction || !b->restitution || !b->linear_damping ||
@@ -495,7 +540,18 @@ int ne_world_upload(NeWorld* w, const NeBodyArrays* b) {
     if (!planes.empty())
         NE_CUDA_TRY(cudaMemcpy(d.planes, planes.data(), planes.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
 
-    derive_grid(w, boundR, shapes);
+    w->nworlds = nworlds;
+    w->wparams.assign(params, params + nworlds);
+    w->wbegin.assign(wbegin, wbegin + nworlds + 1);
+    w->h_bound = boundR;
+    w->h_shape = shapes;
+    std::vector<uint32_t> bw(n ? n : 1, 0);
+    for (uint32_t k = 0; k < nworlds; ++k)
+        for (uint32_t i = wbegin[k]; i < wbegin[k + 1]; ++i) bw[i] = k;
+    dfree(w->d_bw);
+    if ((rc = dalloc(&w->d_bw, bw.size()))) return rc;
+    NE_CUDA_TRY(cudaMemcpy(w->d_bw, bw.data(), bw.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    if ((rc = derive_worlds(w, planes))) return rc;
 
     // Initial capacities; they grow on demand (see ne_world_step).
     if (!w->Pcap) {
@@ -507,6 +563,24 @@ int ne_world_upload(NeWorld* w, const NeBodyArrays* b) {
     w->has_bodies = true;
     std::memset(&w->stats, 0, sizeof(w->stats));
     return NE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ne_world_upload(NeWorld* w, const NeBodyArrays* b) {
+    if (!w || !b) return set_err(NE_ERR_ARG, "NULL argument");
+    const uint32_t range[2] = {0, b->n};
+    return upload_impl(w, &w->p, 1, range, b);
+}
+
+int ne_world_upload_batch(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const uint32_t* world_begin,
+                          const NeBodyArrays* b) {
+    if (!w || !b || !params || !world_begin) return set_err(NE_ERR_ARG, "NULL argument");
+    int rc = upload_impl(w, params, nworlds, world_begin, b);
+    if (rc == NE_OK) w->p = params[0];
+    return rc;
 }
 
 // Pinned host staging for per-step state traffic: 6 records per body
@@ -642,7 +716,7 @@ int ne_world_step(NeWorld* w, uint32_t nsteps) {
             ++w->stage_steps;
         }
         // Shrink the cell-key sort to the bits this step needed.
-        if (!w->p.periodic) {
+        if (w->any_grid) {
             int kb = (((int)c.need_bits + 7) / 8) * 8;
             if (kb >= 8) w->key_bits = kb;
         }

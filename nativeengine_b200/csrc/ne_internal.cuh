@@ -35,13 +35,13 @@ struct Ctl {
     uint32_t abort;          // a capacity or bit budget was exceeded this step
     uint32_t flags;          // bit0: EPA/clip budget overrun
     uint32_t need_bits;      // sort-key bits the cell keys needed
+    uint32_t local_bits;     // widest per-world cell-key layout this step
     uint32_t wsel;           // warm cache buffer holding the previous step
     uint64_t P, S, C;        // pairs, survivors, contacts (totals, even if over capacity)
     uint64_t islands, max_island, epa_cap_hits;
     uint32_t nbig;           // islands solved by the dataflow kernel this step
     uint32_t solve_timeout;  // a bounded dependency wait ran out (error)
     uint32_t wcount[2];      // warm cache entries per buffer
-    long long cmin[3], cmax[3];   // cell coordinate extents (open/reflective grid)
     uint64_t scan_total;     // scratch total of the last scan
 };
 

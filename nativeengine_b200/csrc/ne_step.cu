@@ -49,42 +49,54 @@ __device__ __forceinline__ BodyG load_geom(const DevWorld& d, uint32_t i) {
 
 __device__ __forceinline__ int bitlen_u64(unsigned long long x) { return x ? 64 - __clzll((long long)x) : 0; }
 
-// Per-axis cell coordinate (src/world.cpp:458-466).
-__device__ __forceinline__ long long cell_of(const StepArgs& a, double c, int axis) {
-    if (a.dom.periodic) {
-        long long k = (long long)floor((c + a.dom.half) / a.cell);
-        long long m = a.nc[axis];
+// Per-axis cell coordinate (src/world.cpp:458-466), in world W's grid.
+__device__ __forceinline__ long long cell_of(const WorldP& W, double c, int axis) {
+    if (W.dom.periodic) {
+        long long k = (long long)floor((c + W.dom.half) / W.cell);
+        long long m = W.nc[axis];
         return ((k % m) + m) % m;
     }
-    return (long long)floor(c / a.cell);
+    return (long long)floor(c / W.cell);
 }
 
 // Compact sort key layout: a bijection of the reference's 21-bit-masked cell
 // coordinates (src/world.cpp:467-470) onto as few bits as the occupied range
-// needs, so the radix sort touches only varying digits.
+// needs, so the radix sort touches only varying digits.  In a batch the world
+// index sits above the local key (`prefix`), so cells of different worlds
+// never compare equal.
 struct KeyLayout {
     int bits[3];
     long long base[3];
     long long span[3];   // occupied offsets are [0, span] per axis
     int total;
+    unsigned long long prefix;
 };
 
-__device__ __forceinline__ KeyLayout key_layout(const StepArgs& a, const Ctl* ctl) {
+__device__ __forceinline__ KeyLayout world_layout(const WorldP& W, const long long* ext) {
     KeyLayout L;
     for (int ax = 0; ax < 3; ++ax) {
-        if (a.dom.periodic) {
-            const long long m = a.nc[ax];
+        if (W.dom.periodic) {
+            const long long m = W.nc[ax];
             L.bits[ax] = (m > (1ll << 21)) ? 21 : bitlen_u64((unsigned long long)(m - 1));
             L.base[ax] = 0;
             L.span[ax] = m - 1;
         } else {
-            const long long span = ctl->cmax[ax] - ctl->cmin[ax];
+            const long long span = ext[3 + ax] - ext[ax];
             L.bits[ax] = (span >= (1ll << 21) || span < 0) ? 21 : bitlen_u64((unsigned long long)span);
-            L.base[ax] = ctl->cmin[ax];
+            L.base[ax] = ext[ax];
             L.span[ax] = span;
         }
     }
     L.total = L.bits[0] + L.bits[1] + L.bits[2];
+    L.prefix = 0;
+    return L;
+}
+
+// Layout of world w's keys; local keys of every world use the low
+// `local_bits` bits (the widest world's total).
+__device__ __forceinline__ KeyLayout key_layout(const StepArgs& a, uint32_t w, int local_bits) {
+    KeyLayout L = world_layout(a.wp[w], a.cext + 6 * (size_t)w);
+    L.prefix = (unsigned long long)w << local_bits;
     return L;
 }
 
@@ -94,7 +106,7 @@ __device__ __forceinline__ unsigned long long compact_key(const KeyLayout& L, lo
     unsigned long long x = (unsigned long long)(cx - L.base[0]) & M;
     unsigned long long y = (unsigned long long)(cy - L.base[1]) & M;
     unsigned long long z = (unsigned long long)(cz - L.base[2]) & M;
-    return x | (y << L.bits[0]) | (z << (L.bits[0] + L.bits[1]));
+    return L.prefix | x | (y << L.bits[0]) | (z << (L.bits[0] + L.bits[1]));
 }
 
 // Key of a neighbour cell.  A cell outside the occupied offset range holds no
@@ -115,21 +127,21 @@ __device__ __forceinline__ unsigned long long neighbour_key(const KeyLayout& L, 
     return compact_key(L, cx, cy, cz);
 }
 
-__device__ __forceinline__ long long wrap_cell(const StepArgs& a, long long c, int axis) {
-    if (!a.dom.periodic) return c;
-    const long long m = a.nc[axis];
+__device__ __forceinline__ long long wrap_cell(const WorldP& W, long long c, int axis) {
+    if (!W.dom.periodic) return c;
+    const long long m = W.nc[axis];
     return ((c % m) + m) % m;
 }
 
 // The distinct neighbour keys of a cell (27 offsets; wrapping can alias them).
-__device__ __forceinline__ int neighbour_keys(const StepArgs& a, const KeyLayout& L, long long cx, long long cy,
+__device__ __forceinline__ int neighbour_keys(const WorldP& W, const KeyLayout& L, long long cx, long long cy,
                                               long long cz, unsigned long long* out) {
     int nk = 0;
     for (int dx = -1; dx <= 1; ++dx)
         for (int dy = -1; dy <= 1; ++dy)
             for (int dz = -1; dz <= 1; ++dz) {
-                unsigned long long k = neighbour_key(L, wrap_cell(a, cx + dx, 0), wrap_cell(a, cy + dy, 1),
-                                                     wrap_cell(a, cz + dz, 2));
+                unsigned long long k = neighbour_key(L, wrap_cell(W, cx + dx, 0), wrap_cell(W, cy + dy, 1),
+                                                     wrap_cell(W, cz + dz, 2));
                 bool dup = false;
                 for (int t = 0; t < nk; ++t) dup |= (out[t] == k);
                 if (!dup) out[nk++] = k;
@@ -170,19 +182,25 @@ __device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t* a, uint32_t 
 
 // ---------------------------------------------------------------------------
 
-__global__ void k_step_begin(Ctl* ctl) {
-    ctl->abort = 0;
-    ctl->flags = 0;
-    ctl->need_bits = 0;
-    ctl->P = ctl->S = ctl->C = 0;
-    ctl->islands = 0;
-    ctl->max_island = 0;
-    ctl->epa_cap_hits = 0;
-    ctl->nbig = 0;
-    ctl->solve_timeout = 0;
-    for (int a = 0; a < 3; ++a) {
-        ctl->cmin[a] = 0x7fffffffffffffffll;
-        ctl->cmax[a] = (long long)0x8000000000000000ull;
+__global__ void k_step_begin(Ctl* ctl, long long* ext, uint32_t nworlds) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) {
+        ctl->abort = 0;
+        ctl->flags = 0;
+        ctl->need_bits = 0;
+        ctl->local_bits = 0;
+        ctl->P = ctl->S = ctl->C = 0;
+        ctl->islands = 0;
+        ctl->max_island = 0;
+        ctl->epa_cap_hits = 0;
+        ctl->nbig = 0;
+        ctl->solve_timeout = 0;
+    }
+    if (t < nworlds) {
+        for (int a = 0; a < 3; ++a) {
+            ext[6 * (size_t)t + a] = 0x7fffffffffffffffll;
+            ext[6 * (size_t)t + 3 + a] = (long long)0x8000000000000000ull;
+        }
     }
 }
 
@@ -202,103 +220,131 @@ __device__ __forceinline__ long long warp_max_ll(long long v) {
 }
 
 // World::integrate() (src/world.cpp:373-411) + pre-step snapshot + union-find
-// reset + cell extents of the post-integration positions.
+// reset + cell extents of the post-integration positions (per world).
 __global__ void __launch_bounds__(kT) k_integrate(StepArgs a) {
-    Ctl* ctl = a.d.ctl;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < a.n;
+    const uint32_t w = live ? a.bw[i] : 0xffffffffu;
     long long lo[3] = {0x7fffffffffffffffll, 0x7fffffffffffffffll, 0x7fffffffffffffffll};
     long long hi[3] = {(long long)0x8000000000000000ull, (long long)0x8000000000000000ull,
                        (long long)0x8000000000000000ull};
+    bool track = false;
     if (live) {
         const DevWorld& d = a.d;
+        const WorldP& W = a.wp[w];
         D4 p = d.pos[i], q4 = d.quat[i], v4 = d.vel[i], w4 = d.omg[i], f4 = d.frc[i], t4 = d.trq[i];
         d.s_pos[i] = p; d.s_quat[i] = q4; d.s_vel[i] = v4; d.s_omg[i] = w4; d.s_frc[i] = f4; d.s_trq[i] = t4;
         d.parent[i] = i;
         const uint4 m = d.meta[i];
-        V3 x = v3of(p), v = v3of(v4), w = v3of(w4), F = v3of(f4), T = v3of(t4);
+        V3 x = v3of(p), v = v3of(v4), wv = v3of(w4), F = v3of(f4), T = v3of(t4);
         Q q = qof(q4);
-        const double invM = p.w, dt = a.dt;
+        const double invM = p.w, dt = W.dt;
         if (m.y & NE_BODY_KINEMATIC) {
             x = x + v * dt;
-            q = integrate_orientation(q, w, dt);
+            q = integrate_orientation(q, wv, dt);
         } else if (invM <= 0.0) {
         } else {
             const D4 I = d.inert[i], g = d.geom[i], mt = d.mat[i];
             const V3 invI = v3of(I);
-            v = v + (a.g * g.z + F * invM) * dt;
+            v = v + (W.g * g.z + F * invM) * dt;
             x = x + v * dt;
-            V3 L = angular_momentum(q, invI, w);
+            V3 L = angular_momentum(q, invI, wv);
             L = L + T * dt;
-            q = integrate_orientation(q, w, dt);
-            w = apply_inv_inertia(q, invI, L);
+            q = integrate_orientation(q, wv, dt);
+            wv = apply_inv_inertia(q, invI, L);
             if (mt.z > 0.0) v = v * (1.0 / (1.0 + mt.z * dt));
-            if (mt.w > 0.0) w = w * (1.0 / (1.0 + mt.w * dt));
+            if (mt.w > 0.0) wv = wv * (1.0 / (1.0 + mt.w * dt));
         }
         F = mk(0.0, 0.0, 0.0);
         T = F;
         d.pos[i] = d4of(x, invM);
         d.quat[i] = d4ofq(q);
         d.vel[i] = d4of(v, 0.0);
-        d.omg[i] = d4of(w, 0.0);
+        d.omg[i] = d4of(wv, 0.0);
         d.frc[i] = d4of(F, 0.0);
         d.trq[i] = d4of(T, 0.0);
-        if (!a.brute && !a.dom.periodic && !grid_excluded((int)m.x)) {
+        if (!W.brute && !W.dom.periodic && !grid_excluded((int)m.x)) {
             const double c[3] = {x.x, x.y, x.z};
-            for (int ax = 0; ax < 3; ++ax) lo[ax] = hi[ax] = cell_of(a, c[ax], ax);
+            for (int ax = 0; ax < 3; ++ax) lo[ax] = hi[ax] = cell_of(W, c[ax], ax);
+            track = true;
         }
     }
-    if (!a.brute && !a.dom.periodic) {
+    // Extents: one atomic per warp when the warp's bodies share a world.
+    const uint32_t w0 = __shfl_sync(0xffffffffu, w, 0);
+    if (__all_sync(0xffffffffu, w == w0)) {
+        if (!__any_sync(0xffffffffu, track)) return;
         for (int ax = 0; ax < 3; ++ax) {
             long long mn = warp_min_ll(lo[ax]), mx = warp_max_ll(hi[ax]);
             if ((threadIdx.x & 31) == 0 && mn <= mx) {
-                atomicMin(&ctl->cmin[ax], mn);
-                atomicMax(&ctl->cmax[ax], mx);
+                atomicMin(&a.cext[6 * (size_t)w0 + ax], mn);
+                atomicMax(&a.cext[6 * (size_t)w0 + 3 + ax], mx);
             }
+        }
+    } else if (track) {
+        for (int ax = 0; ax < 3; ++ax) {
+            atomicMin(&a.cext[6 * (size_t)w + ax], lo[ax]);
+            atomicMax(&a.cext[6 * (size_t)w + 3 + ax], hi[ax]);
         }
     }
 }
 
-// Sort keys of the grid cells; grid-excluded bodies get a sentinel that sorts
-// after every real key.
+// Key bits each world's grid needs; the widest decides the local key width.
+__global__ void __launch_bounds__(kT) k_world_layout(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= a.nworlds) return;
+    const WorldP& W = a.wp[w];
+    if (W.brute) return;
+    const KeyLayout L = world_layout(W, a.cext + 6 * (size_t)w);
+    atomicMax(&ctl->local_bits, (uint32_t)L.total);
+}
+
+// Sort keys of the grid cells; grid-excluded bodies and bodies of
+// brute-force worlds get a sentinel that sorts after every real key.
 __global__ void __launch_bounds__(kT) k_cell_keys(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const KeyLayout L = key_layout(a, ctl);
+    const int lb = (int)ctl->local_bits;
+    const int total = a.world_bits + lb;
     if (i == 0) {
-        ctl->need_bits = (uint32_t)(L.total + 1);
-        if (L.total + 1 > a.key_bits) ctl->abort = 1;
+        ctl->need_bits = (uint32_t)(total + 1);
+        if (total + 1 > a.key_bits) ctl->abort = 1;
     }
     if (i >= a.n) return;
+    const uint32_t w = a.bw[i];
+    const WorldP& W = a.wp[w];
     const D4 p = a.d.pos[i];
     const int shape = (int)a.d.meta[i].x;
     unsigned long long k;
-    if (grid_excluded(shape)) {
-        k = 1ull << L.total;
+    if (W.brute || grid_excluded(shape)) {
+        k = 1ull << total;
     } else {
-        k = compact_key(L, cell_of(a, p.x, 0), cell_of(a, p.y, 1), cell_of(a, p.z, 2));
+        const KeyLayout L = key_layout(a, w, lb);
+        k = compact_key(L, cell_of(W, p.x, 0), cell_of(W, p.y, 1), cell_of(W, p.z, 2));
     }
     a.d.key[0][i] = k;
     a.d.val[0][i] = i;
 }
 
 // Number of partners j > i of body i (the sorted unique pair list is the CSR
-// of these partner lists).
+// of these partner lists).  Partners are always in body i's world.
 __global__ void __launch_bounds__(kT) k_pair_count(StepArgs a, int kb) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const DevWorld& d = a.d;
-    if (a.brute || grid_excluded((int)d.meta[i].x)) {
-        d.bcnt[i] = a.n - 1 - i;
+    const uint32_t w = a.bw[i];
+    const WorldP& W = a.wp[w];
+    if (W.brute || grid_excluded((int)d.meta[i].x)) {
+        d.bcnt[i] = W.end - 1 - i;
         return;
     }
-    const KeyLayout L = key_layout(a, ctl);
+    const KeyLayout L = key_layout(a, w, (int)ctl->local_bits);
     const D4 p = d.pos[i];
     unsigned long long nk[27];
-    const int m = neighbour_keys(a, L, cell_of(a, p.x, 0), cell_of(a, p.y, 1), cell_of(a, p.z, 2), nk);
+    const int m = neighbour_keys(W, L, cell_of(W, p.x, 0), cell_of(W, p.y, 1), cell_of(W, p.z, 2), nk);
     const unsigned long long* keys = d.key[kb];
     const uint32_t* vals = d.val[kb];
     uint32_t cnt = 0;
@@ -309,16 +355,16 @@ __global__ void __launch_bounds__(kT) k_pair_count(StepArgs a, int kb) {
         uint32_t s = upper_bound_u32(vals, lo, hi, i);
         cnt += hi - s;
     }
-    cnt += a.nplanes - upper_bound_u32(d.planes, 0, a.nplanes, i);
+    cnt += W.plane_end - upper_bound_u32(d.planes, W.plane_begin, W.plane_end, i);
     d.bcnt[i] = cnt;
 }
 
 // Writes body i's sorted partner list at its CSR offset.  One warp per body.
 // The partner candidates are up to 27 sorted runs (one per distinct
-// neighbour cell; members with index > i) plus the sorted run of planes > i.
-// Lanes split the concatenated candidates evenly; each candidate's output rank
-// is its index in its own run plus the number of smaller candidates in the
-// other runs (all candidates are distinct body indices).
+// neighbour cell; members with index > i) plus the sorted run of the world's
+// planes > i.  Lanes split the concatenated candidates evenly; each
+// candidate's output rank is its index in its own run plus the number of
+// smaller candidates in the other runs (all candidates are distinct bodies).
 __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
@@ -331,18 +377,20 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
     const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= a.n) return;
     const DevWorld& d = a.d;
+    const uint32_t w = a.bw[i];
+    const WorldP& W = a.wp[w];
     const uint32_t base = d.boff[i];
-    if (a.brute || grid_excluded((int)d.meta[i].x)) {
-        const uint32_t cnt = a.n - 1 - i;
+    if (W.brute || grid_excluded((int)d.meta[i].x)) {
+        const uint32_t cnt = W.end - 1 - i;
         for (uint32_t k = lane; k < cnt; k += 32) {
             d.pair_i[base + k] = i;
             d.pair_j[base + k] = i + 1 + k;
         }
         return;
     }
-    const KeyLayout L = key_layout(a, ctl);
+    const KeyLayout L = key_layout(a, w, (int)ctl->local_bits);
     const D4 p = d.pos[i];
-    const long long cx = cell_of(a, p.x, 0), cy = cell_of(a, p.y, 1), cz = cell_of(a, p.z, 2);
+    const long long cx = cell_of(W, p.x, 0), cy = cell_of(W, p.y, 1), cz = cell_of(W, p.z, 2);
     const unsigned long long* keys = d.key[kb];
     const uint32_t* vals = d.val[kb];
     // Lane t < 27 takes neighbour offset t (duplicates from wrap aliasing keep
@@ -350,8 +398,8 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
     uint32_t rlo = 0, rhi = 0;
     if (lane < 27) {
         const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
-        unsigned long long k = neighbour_key(L, wrap_cell(a, cx + dx, 0), wrap_cell(a, cy + dy, 1),
-                                             wrap_cell(a, cz + dz, 2));
+        unsigned long long k = neighbour_key(L, wrap_cell(W, cx + dx, 0), wrap_cell(W, cy + dy, 1),
+                                             wrap_cell(W, cz + dz, 2));
         const uint32_t grp = __match_any_sync(0x07ffffffu, k);
         if (lane == __ffs(grp) - 1) {
             uint32_t lo = lower_bound_u64(keys, 0, a.n, k);
@@ -360,8 +408,8 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
             rhi = hi;
         }
     } else if (lane == 27) {
-        rlo = upper_bound_u32(d.planes, 0, a.nplanes, i);
-        rhi = a.nplanes;
+        rlo = upper_bound_u32(d.planes, W.plane_begin, W.plane_end, i);
+        rhi = W.plane_end;
     }
     // Compact the non-empty runs into shared memory, in lane order.
     const uint32_t len = rhi - rlo;
@@ -434,7 +482,7 @@ __global__ void __launch_bounds__(kT) k_pair_cull(StepArgs a) {
         if (keep && sa != SH_PLANE && sb != SH_PLANE) {
             // Bounding spheres about the centres (nearest image).
             const double ra = d.inert[i].w, rb = d.inert[j].w;
-            const V3 dd = min_image(a.dom, mk(pb.x - pa.x, pb.y - pa.y, pb.z - pa.z));
+            const V3 dd = min_image(a.wp[a.bw[i]].dom, mk(pb.x - pa.x, pb.y - pa.y, pb.z - pa.z));
             const double r = (ra + rb) * (1.0 + 1e-9) + 1e-9;
             if (norm2(dd) > r * r) keep = 0;
             // Box vs bounding sphere: distance from the sphere centre to the box.
@@ -484,11 +532,12 @@ __global__ void __launch_bounds__(128) k_narrowphase(StepArgs a) {
     const BodyG A = load_geom(d, i), B = load_geom(d, j);
     EpaScratch S;
     int fl = 0;
-    Contact c = detect_contact(A, B, a.dom, S, fl);
+    const Domain dom = a.wp[a.bw[i]].dom;
+    Contact c = detect_contact(A, B, dom, S, fl);
     uint32_t cnt = 0;
     if (c.hit) {
         if (A.shape == SH_BOX && B.shape == SH_BOX) {
-            Manifold m = box_box_manifold(A, B, c.normal, a.dom, fl);
+            Manifold m = box_box_manifold(A, B, c.normal, dom, fl);
             for (int k = 0; k < m.count; ++k) {
                 d.cn[4 * s + k] = d4of(c.normal, m.depth[k]);
                 d.cp[4 * s + k] = d4of(m.point[k], 0.0);
@@ -573,10 +622,11 @@ __global__ void __launch_bounds__(kT) k_constraint_build(StepArgs a) {
     const V3 xa = v3of(pa), xb = v3of(pb);
     const V3 va = v3of(d.vel[i]), vb = v3of(d.vel[j]), wa = v3of(d.omg[i]), wb = v3of(d.omg[j]);
     const D4 ma = d.mat[i], mb = d.mat[j];
-    const double ea = ma.y < 0 ? a.restitution : ma.y, eb = mb.y < 0 ? a.restitution : mb.y;
-    const double fa = ma.x < 0 ? a.friction : ma.x, fb = mb.x < 0 ? a.friction : mb.x;
-    const double e = combine_mat(a.rcomb, ea, eb);
-    const double mu = combine_mat(a.fcomb, fa, fb);
+    const WorldP& W = a.wp[a.bw[i]];
+    const double ea = ma.y < 0 ? W.restitution : ma.y, eb = mb.y < 0 ? W.restitution : mb.y;
+    const double fa = ma.x < 0 ? W.friction : ma.x, fb = mb.x < 0 ? W.friction : mb.x;
+    const double e = combine_mat(W.rcomb, ea, eb);
+    const double mu = combine_mat(W.fcomb, fa, fb);
     const uint32_t fla = d.meta[i].y, flb = d.meta[j].y;
     if ((fla & kFlagMutable) && (flb & kFlagMutable)) uf_union(d.parent, i, j);
     const unsigned long long key = ((unsigned long long)i << 32) | (unsigned long long)j;
@@ -589,8 +639,8 @@ __global__ void __launch_bounds__(kT) k_constraint_build(StepArgs a) {
         const uint32_t c = c0 + k;
         const D4 cn = d.cn[4 * s + k];
         const V3 n = v3of(cn), pt = v3of(d.cp[4 * s + k]);
-        const V3 rA = min_image(a.dom, pt - xa);
-        const V3 rB = min_image(a.dom, pt - xb);
+        const V3 rA = min_image(W.dom, pt - xa);
+        const V3 rB = min_image(W.dom, pt - xb);
         const V3 vc = (va + cross(wa, rA)) - (vb + cross(wb, rB));
         const double vn = dot(vc, n);
         const double restBias = (vn < -0.5) ? -e * vn : 0.0;
@@ -833,7 +883,8 @@ __global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
     for (int it = 0; it < 8; ++it)
         for (uint32_t k = s; k < e; ++k) sweep_item(d, ord[k]);
     double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
-    for (uint32_t k = s; k < e; ++k) correct_item(d, ord[k], a.beta, wout);
+    const double beta = a.wp[a.bw[d.ci[ord[s]]]].beta;
+    for (uint32_t k = s; k < e; ++k) correct_item(d, ord[k], beta, wout);
 }
 
 // A warp that sees no update complete for this long gives up and reports
@@ -932,6 +983,7 @@ __global__ void __launch_bounds__(kBigThreads) k_island_solve_big(StepArgs a, in
         const uint32_t s = d.istart[t], e = d.istart[t + 1];
         const uint32_t m = e - s;
         const uint32_t total = 10u * m;
+        const double beta = a.wp[a.bw[d.ci[ord[s]]]].beta;
         uint32_t* cnt = d.bcnt10 + 10u * s;      // per-island slices of the 10*C scratch
         uint32_t* queue = d.bq10 + 10u * s;
         if (threadIdx.x == 0) { s_fail = 0; s_head = 0; s_tail = 0; }
@@ -964,7 +1016,7 @@ __global__ void __launch_bounds__(kBigThreads) k_island_solve_big(StepArgs a, in
                 } else if (it.p <= 8) {
                     sweep_item(d, it.c);
                 } else {
-                    correct_item(d, it.c, a.beta, wout);
+                    correct_item(d, it.c, beta, wout);
                 }
                 const uint32_t si = it.mi ? big_successor(d, rv, it, 0, it.i, s, m) : kEmpty;
                 const uint32_t sj = it.mj ? big_successor(d, rv, it, 1, it.j, s, m) : kEmpty;
@@ -1003,17 +1055,18 @@ __global__ void __launch_bounds__(kT) k_boundary(StepArgs a) {
     const DevWorld& d = a.d;
     D4 p = d.pos[i];
     if (!(p.w > 0.0)) return;
-    if (a.dom.periodic) {
-        V3 x = wrap(a.dom, v3of(p));
+    const WorldP& W = a.wp[a.bw[i]];
+    if (W.dom.periodic) {
+        V3 x = wrap(W.dom, v3of(p));
         d.pos[i] = d4of(x, p.w);
         return;
     }
-    if (a.open_boundary) return;
+    if (W.open_boundary) return;
     BodyG b = load_geom(d, i);
     D4 v4 = d.vel[i];
     double px[3] = {p.x, p.y, p.z};
     double pv[3] = {v4.x, v4.y, v4.z};
-    const double h = a.dom.half;
+    const double h = W.dom.half;
     for (int axis = 0; axis < 3; ++axis) {
         for (int sgn = -1; sgn <= 1; sgn += 2) {
             V3 outward = mk(axis == 0 ? double(sgn) : 0.0, axis == 1 ? double(sgn) : 0.0,
@@ -1024,7 +1077,7 @@ __global__ void __launch_bounds__(kT) k_boundary(StepArgs a) {
             double pen = coord - h;
             if (pen > 0.0) {
                 px[axis] -= double(sgn) * pen;
-                if (pv[axis] * sgn > 0.0) pv[axis] = -a.restitution * pv[axis];
+                if (pv[axis] * sgn > 0.0) pv[axis] = -W.restitution * pv[axis];
             }
         }
     }
@@ -1057,13 +1110,14 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
         if (ev) cudaEventRecord(ev[k], st);
     };
     mark(0);
-    k_step_begin<<<1, 1, 0, st>>>(ctl); ++L;
+    k_step_begin<<<blocks_for(a.nworlds, kT), kT, 0, st>>>(ctl, a.cext, a.nworlds); ++L;
     k_integrate<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
 
     mark(1);
     // Broadphase: cell keys -> stable sort -> per-body partner counts -> CSR.
     int kb = 0;
-    if (!a.brute) {
+    if (a.any_grid) {
+        k_world_layout<<<blocks_for(a.nworlds, kT), kT, 0, st>>>(a); ++L;
         k_cell_keys<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
         unsigned long long* keys[2] = {d.key[0], d.key[1]};
         uint32_t* vals[2] = {d.val[0], d.val[1]};

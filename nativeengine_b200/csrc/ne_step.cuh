@@ -1,26 +1,41 @@
-// ne_step.cuh -- by-value launch arguments of the step kernels.
+// ne_step.cuh -- launch arguments of the step kernels.
+//
+// One device world holds one or more independent simulation worlds (a
+// batch).  Bodies of world w occupy the index range [begin, end); no pair,
+// contact or island ever spans two worlds.  A single ne::World is a batch of
+// one, so it runs exactly the same kernels.
 #pragma once
 
 #include "ne_internal.cuh"
 
 namespace neb {
 
-struct StepArgs {
-    DevWorld d;
-    uint32_t n;              // bodies
+// Per-world configuration: ne::World's fields (src/world.hpp:75-126) plus the
+// broadphase constants World::broadphasePairs() derives (src/world.cpp:427-457).
+struct WorldP {
     Domain dom;              // Box (half, periodic)
     double dt, restitution, friction, beta;
     V3 g;                    // gravity
     int rcomb, fcomb;        // material combine modes
-    int warm;                // World::warmStart
     int open_boundary;
-    // broadphase constants (fixed per upload: cell = 2 * max bounding radius)
-    double cell;
-    long long nc[3];
     int brute;               // forceBruteForce || n < 64 || cell < 1e-9
-    uint32_t nplanes;
+    double cell;             // 2 * max bounding radius
+    long long nc[3];         // periodic cell counts
+    uint32_t begin, end;     // body range
+    uint32_t plane_begin, plane_end;   // range of this world's grid-excluded bodies in DevWorld::planes
+};
+
+struct StepArgs {
+    DevWorld d;
+    uint32_t n;              // bodies, all worlds
+    uint32_t nworlds;
+    int world_bits;          // bits of a world index in a cell key
+    const WorldP* wp;        // [nworlds], device
+    const uint32_t* bw;      // [n] world of each body, device
+    long long* cext;         // [6 * nworlds] cell extents (min xyz, max xyz) per world
     int key_bits;            // bits the cell-key sort covers this step
-    // capacities
+    int any_grid;            // some world uses the grid (else every world is brute force)
+    int warm;                // warm starting (one setting for the whole batch)
     uint64_t Pcap, Scap, Ccap;
     int num_sms;
 };

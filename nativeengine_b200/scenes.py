@@ -168,6 +168,47 @@ def _hull_volume(pts: np.ndarray) -> float:
         return float(np.prod(ext)) * 0.3
 
 
+def batch_mix(nworlds: int = 2048, lo: int = 16, hi: int = 2048, seed: int = 4, dt: float = 1.0 / 60.0):
+    """Independent worlds for the batched form: body counts log-uniform in
+    [lo, hi]; each world is (by a seeded coin) a box pile -- static ground box
+    plus ceil(n^(1/3))^3 lattice truncated to n boxes -- or a periodic sphere
+    gas at the gas_1000 density (edge 25*(n/1000)^(1/3)).  Returns
+    (params_list, BodyArrays, world_begin, kinds)."""
+    from .bodies import concat
+    rng = _rng(seed)
+    params, parts, kinds = [], [], []
+    for w in range(nworlds):
+        n = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
+        wseed = int(rng.integers(1, 2**31 - 1))
+        if rng.integers(0, 2) == 0:
+            side = int(math.ceil(n ** (1.0 / 3.0) - 1e-9))
+            p, b = _pile_truncated(side, n, wseed, dt)
+            kinds.append("box_pile")
+        else:
+            half = 12.5 * (n / 1000.0) ** (1.0 / 3.0)
+            p, b = gas(n=n, half=half, seed=wseed, dt=dt)
+            kinds.append("gas")
+        params.append(p)
+        parts.append(b)
+    bodies, begin = concat(parts)
+    return params, bodies, begin, kinds
+
+
+def _pile_truncated(side, n, seed, dt):
+    rng = _rng(seed)
+    bodies: List[Body] = [make_static(make_box((0.0, -1.0, 0.0), (1.0, 0.0, 0.0, 0.0), (50.0, 1.0, 50.0), 1.0))]
+    c = (side - 1) / 2.0
+    for i in range(side):
+        for j in range(side):
+            for k in range(side):
+                if len(bodies) > n:
+                    break
+                he = tuple(rng.uniform(0.25, 0.75, 3))
+                bodies.append(make_box(((i - c) * 1.6, 2.0 + j * 1.6, (k - c) * 1.6), random_quat(rng), he, 1.0))
+    params = default_params(open_boundary=1, gravity=(0.0, -9.81, 0.0), dt=dt, friction=0.5, restitution=0.2)
+    return params, BodyArrays(bodies)
+
+
 # ---- small worlds for parity tests -----------------------------------------
 
 def small_gas(n=50, half=8.0, periodic=True, seed=999, dt=5e-3, spin=True):

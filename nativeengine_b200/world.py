@@ -57,6 +57,19 @@ class DeviceWorld:
         self.n = bodies.n
         _ffi.check(self._lib.ne_world_upload(self._h, C.byref(bodies.c)), "ne_world_upload")
 
+    def upload_batch(self, params_list, bodies: BodyArrays, world_begin):
+        """Upload a batch: world k owns bodies [world_begin[k], world_begin[k+1])."""
+        self._bodies = bodies
+        self.n = bodies.n
+        nw = len(params_list)
+        arr = (_ffi.NeWorldParams * nw)(*params_list)
+        self._batch_params = arr
+        wb = np.ascontiguousarray(world_begin, dtype=np.uint32)
+        assert wb.shape == (nw + 1,)
+        self._wb = wb
+        _ffi.check(self._lib.ne_world_upload_batch(self._h, arr, nw, _ptr(wb), C.byref(bodies.c)),
+                   "ne_world_upload_batch")
+
     def upload_state(self, x=None, q=None, v=None, w=None):
         arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (x, q, v, w)]
         _ffi.check(self._lib.ne_world_upload_state(self._h, *[_ptr(a) for a in arrs]), "ne_world_upload_state")
