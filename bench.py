@@ -33,6 +33,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -59,6 +61,12 @@ def _cfg_gas():
     return scenes.gas()
 
 
+def _cfg_batch():
+    from nativeengine_b200 import scenes
+    params, bodies, begin, kinds = scenes.batch_mix()
+    return params, bodies, begin
+
+
 def _cfg_granular():
     from nativeengine_b200 import scenes
     return scenes.granular_mix(n=65536, max_attempts=2000)
@@ -69,13 +77,17 @@ CONFIGS = {
     "box_pile_8": (_cfg_box_pile_8, "box_pile_512: as box_pile_4096 on an 8^3 lattice (profiling case)"),
     "gas": (_cfg_gas, "gas_1000: periodic elastic gas, 1,000 spheres r=0.5 m=1, L=25, v~N(0,1), e=1, mu=0, "
                       "g=0, dt=1/60 (seed 1)"),
+    "batch": (_cfg_batch, "batch_2048: 2,048 independent worlds, body counts log-uniform in [16, 2048] "
+                          "(~879k bodies), each a box pile (as box_pile at its size) or a periodic sphere gas "
+                          "(as gas_1000 at its size), chosen 50/50 from seed 4; all worlds in one launch "
+                          "sequence"),
     "granular": (_cfg_granular, "granular_65536: periodic mix of spheres/capsules/cylinders/12-point hulls "
                                 "(types by index mod 4), exact-overlap random sequential placement at the "
                                 "densest box that places all bodies (true-volume packing fraction ~0.19), "
                                 "v~N(0,0.5), mu=0.3, e=0.5, g=0, dt=1/60 (seed 3)"),
 }
 # Reference-CPU sample per config: physics steps timed on one host core.
-CPU_SAMPLE_STEPS = {"box_pile": 3, "box_pile_8": 20, "gas": 2000, "granular": 2}
+CPU_SAMPLE_STEPS = {"box_pile": 3, "box_pile_8": 20, "gas": 2000, "granular": 2, "batch": 2}
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "solve_box_pile_512.md")
 
 
@@ -185,6 +197,36 @@ def cpu_baseline_reference(config: str, params, bodies):
             "sample": f"first {steps} steps of {config} ({bodies.n} bodies) on one host core ({dt:.1f} s)"}
 
 
+def cpu_baseline_batch(params, bodies, begin, worlds: int = 64):
+    """The reference on the first `worlds` worlds of the batch (one host core,
+    one World at a time, as the reference steps them), 2 steps each."""
+    from nativeengine_b200.bodies import BodyArrays
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    steps = CPU_SAMPLE_STEPS["batch"]
+    work, t = 0, 0.0
+    for k in range(min(worlds, len(params))):
+        b0, b1 = int(begin[k]), int(begin[k + 1])
+        sub = BodyArrays.__new__(BodyArrays)
+        for key, v in bodies.__dict__.items():
+            if isinstance(v, np.ndarray) and v.shape[:1] == (bodies.n,):
+                setattr(sub, key, np.ascontiguousarray(v[b0:b1]))
+        sub.n = b1 - b0
+        sub.verts, sub.n_verts = bodies.verts, bodies.n_verts
+        sub.nocollide, sub.n_nocollide = bodies.nocollide, 0
+        sub.nocollide_count = np.zeros(sub.n, np.uint32)
+        sub._c = None
+        ora = O.RefOracle(params[k], sub)
+        t0 = time.perf_counter()
+        ora.step_plain(steps)
+        t += time.perf_counter() - t0
+        work += sub.n * steps
+    return {"value": work / t, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"first {min(worlds, len(params))} worlds of batch_2048, {steps} steps each, one host core "
+                      f"({t:.1f} s)"}
+
+
 def _ref_worker(args):
     steps, q = args
     sys.path.insert(0, ROOT)
@@ -249,9 +291,15 @@ def run_ours(args):
     from nativeengine_b200 import DeviceWorld
 
     make, workload = CONFIGS[args.config]
-    params, bodies = make()
+    made = make()
+    params, bodies = made[0], made[1]
+    begin = made[2] if len(made) > 2 else None
     n = bodies.n
-    dev = DeviceWorld(params, bodies.copy())
+    if begin is None:
+        dev = DeviceWorld(params, bodies.copy(), record=False)
+    else:
+        dev = DeviceWorld(params[0], None, record=False)
+        dev.upload_batch(params, bodies.copy(), begin)
     stream = torch.cuda.ExternalStream(dev.stream_handle())
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
 
@@ -265,7 +313,10 @@ def run_ours(args):
         torch.cuda.synchronize()
 
     def timed_run(host_io: bool):
-        dev.upload(bodies.copy())
+        if begin is None:
+            dev.upload(bodies.copy())
+        else:
+            dev.upload_batch(params, bodies.copy(), begin)
         dev.reset_warm_cache()
         st = bodies.state()
         K = args.steps
@@ -350,7 +401,10 @@ def run_ours(args):
                               "achieved_gbs_mean": step_bytes / (t_dev / K) / 1e9},
         }
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline_reference(args.config, params, bodies)
+            if begin is None:
+                line["cpu_baseline"] = cpu_baseline_reference(args.config, params, bodies)
+            else:
+                line["cpu_baseline"] = cpu_baseline_batch(params, bodies, begin)
         print(json.dumps(line))
     dev.close()
     if world > 1:

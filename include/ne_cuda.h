@@ -154,7 +154,8 @@ typedef struct NeContactArrays {
 
 /* Per-step counters of the last successful step. */
 typedef struct NeStepStats {
-    uint64_t pairs;          /* broadphase candidate pairs (sorted, unique)   */
+    uint64_t pairs;          /* reference-rule broadphase pairs when recording,
+                                else the internal candidate pairs             */
     uint64_t survivors;      /* pairs passing filters + bounding-sphere cull  */
     uint64_t contacts;       /* contact constraints                           */
     uint64_t islands;        /* solver islands (connected components)         */
@@ -162,6 +163,7 @@ typedef struct NeStepStats {
     uint64_t epa_cap_hits;   /* EPA runs that stopped at the 64-iteration cap */
     uint64_t steps;          /* steps taken since upload                      */
     uint64_t retries;        /* steps re-run after growing a device buffer    */
+    uint64_t candidates;     /* pairs the internal grid handed to the cull    */
 } NeStepStats;
 
 typedef struct NeWorld NeWorld;
@@ -205,9 +207,18 @@ int ne_world_reset_warm_cache(NeWorld* world);
 
 /* Introspection of the last step (parity probes). */
 int ne_world_stats(const NeWorld* world, NeStepStats* out);
+/* Recording of step intermediates.  With NE_RECORD_PAIRS set, each step also
+ * builds the pair list exactly as World::broadphasePairs() does
+ * (src/world.cpp:424-501) for ne_world_pairs.  Off by default: internally the
+ * step pairs bodies whose bounding radius is far above their world's typical
+ * size (a ground box) with everyone, like planes, and grids the rest with a
+ * cell sized for them; every pair that can pass the bounding-volume cull is
+ * still examined, so contacts and results do not depend on this setting. */
+#define NE_RECORD_PAIRS 1u
+int ne_world_set_record(NeWorld* world, uint32_t flags);
 /* Broadphase pairs of the last step, as World::broadphasePairs() returned them
  * (src/world.cpp:424-501): sorted by (i, j), unique, i < j.  *count receives
- * the total; at most cap pairs are written. */
+ * the total; at most cap pairs are written.  Needs NE_RECORD_PAIRS. */
 int ne_world_pairs(NeWorld* world, uint32_t* i, uint32_t* j, uint64_t cap,
                    uint64_t* count);
 /* Contacts of the last step in solver order; *count receives the total. */

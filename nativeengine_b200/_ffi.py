@@ -23,6 +23,7 @@ NE_ERR_TIMEOUT = 5
 NE_ERR_NUMERIC = 6
 NE_ERR_NO_DEVICE = 7
 NUM_STAGES = 8
+RECORD_PAIRS = 1
 NOALLOC_MAX_BODIES = 2048
 NOALLOC_MAX_PAIRS = 262144
 
@@ -89,7 +90,7 @@ class NeStepStats(C.Structure):
     _fields_ = [
         ("pairs", C.c_uint64), ("survivors", C.c_uint64), ("contacts", C.c_uint64),
         ("islands", C.c_uint64), ("max_island", C.c_uint64), ("epa_cap_hits", C.c_uint64),
-        ("steps", C.c_uint64), ("retries", C.c_uint64),
+        ("steps", C.c_uint64), ("retries", C.c_uint64), ("candidates", C.c_uint64),
     ]
 
 
@@ -112,6 +113,7 @@ EXPORTS = {
     "ne_world_islands": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "ne_world_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "ne_world_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "ne_world_set_record": (C.c_int, [C.c_void_p, C.c_uint32]),
     "ne_world_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "ne_world_stage_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "ne_stage_name": (C.c_char_p, [C.c_int]),

@@ -8,6 +8,7 @@
 // restores the pre-step snapshot that k_integrate took, grows the buffers and
 // runs the step again -- so growth never changes the result, and steady-state
 // steps cost one small device->host read of the control block.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -48,7 +49,7 @@ void dfree(T*& p) {
     p = nullptr;
 }
 
-inline size_t grow_to(uint64_t need) { return (size_t)(need + need / 4 + 1024); }
+inline size_t grow_to(uint64_t need) { return (size_t)(need + need / 2 + 4096); }
 
 }  // namespace
 
@@ -76,6 +77,9 @@ struct NeWorld {
     long long* d_cext = nullptr;          // per-world cell extents
     int world_bits = 0;
     int any_grid = 0;
+    std::vector<uint8_t> h_large;         // body flagged large (internal grid)
+    uint32_t record = 0;                  // NE_RECORD_* flags
+    uint64_t Rcap = 0;                    // capacity of the recorded pair list
     int key_bits = 64;
     int num_sms = 148;
     // capacities (entries)
@@ -109,6 +113,16 @@ void free_body_arrays(NeWorld* w) {
 void free_pair_arrays(NeWorld* w) {
     neb::DevWorld& d = w->d;
     dfree(d.pair_i); dfree(d.pair_j); dfree(d.pflag); dfree(d.poff);
+}
+
+int alloc_rec(NeWorld* w, uint64_t cap) {
+    neb::DevWorld& d = w->d;
+    dfree(d.rec_i);
+    dfree(d.rec_j);
+    int rc;
+    if ((rc = dalloc(&d.rec_i, cap)) || (rc = dalloc(&d.rec_j, cap))) return rc;
+    w->Rcap = cap;
+    return NE_OK;
 }
 
 void free_surv_arrays(NeWorld* w) {
@@ -213,9 +227,11 @@ neb::StepArgs make_args(const NeWorld* w) {
     a.key_bits = w->key_bits;
     a.any_grid = w->any_grid;
     a.warm = w->wparams.empty() ? (w->p.warm_start ? 1 : 0) : (w->wparams[0].warm_start ? 1 : 0);
+    a.record = (w->record & NE_RECORD_PAIRS) ? 1 : 0;
     a.Pcap = w->Pcap;
     a.Scap = w->Scap;
     a.Ccap = w->Ccap;
+    a.Rcap = w->Rcap;
     a.num_sms = w->num_sms;
     return a;
 }
@@ -236,6 +252,10 @@ int check_params(const NeWorldParams* p) {
 // cell-key sort needs when every grid world is periodic.
 int derive_worlds(NeWorld* w, const std::vector<uint32_t>& planes) {
     const uint32_t nw = w->nworlds;
+    std::vector<uint32_t> xlist;
+    for (uint32_t i = 0; i < w->n; ++i)
+        if (w->h_shape[i] == NE_SHAPE_PLANE || w->h_shape[i] == NE_SHAPE_MESH || w->h_large[i]) xlist.push_back(i);
+    size_t xk = 0;
     w->h_wp.assign(nw, neb::WorldP{});
     w->any_grid = 0;
     int local_bits = 0;
@@ -275,7 +295,43 @@ int derive_worlds(NeWorld* w, const std::vector<uint32_t>& planes) {
         W.plane_begin = (uint32_t)pk;
         while (pk < planes.size() && planes[pk] < W.end) ++pk;
         W.plane_end = (uint32_t)pk;
-        if (!W.brute) {
+        // Internal grid: large bodies are paired with everyone (like planes),
+        // so the cell only has to cover the remaining bodies.  The cell exceeds
+        // every bounding-sphere distance the cull keeps ((ra + rb)(1 + 1e-9) +
+        // 1e-9), so each pair the cull can keep is still a candidate and the
+        // surviving pairs -- hence contacts and results -- are those of the
+        // reference's grid.
+        double maxS = 0.0;
+        for (uint32_t i = W.begin; i < W.end; ++i) {
+            if (w->h_shape[i] == NE_SHAPE_PLANE || w->h_shape[i] == NE_SHAPE_MESH || w->h_large[i]) continue;
+            maxS = (maxS < w->h_bound[i]) ? w->h_bound[i] : maxS;
+        }
+        W.fcell = 2.0 * maxS * (1.0 + 1e-8) + 1e-8;
+        W.fbrute = (W.brute || maxS <= 0.0) ? 1 : 0;
+        W.fnc[0] = W.fnc[1] = W.fnc[2] = 1;
+        if (p.periodic && !W.fbrute) {
+            const double L = 2.0 * p.half;
+            for (int a = 0; a < 3; ++a) {
+                long long m = (long long)std::floor(L / W.fcell);
+                W.fnc[a] = m < 1 ? 1 : m;
+            }
+        }
+        while (xk < xlist.size() && xlist[xk] < W.begin) ++xk;
+        W.xl_begin = (uint32_t)xk;
+        while (xk < xlist.size() && xlist[xk] < W.end) ++xk;
+        W.xl_end = (uint32_t)xk;
+        if (!W.fbrute && p.periodic) {
+            int bits = 0;
+            for (int a = 0; a < 3; ++a) {
+                long long m = W.fnc[a];
+                int b = 0;
+                if (m > (1ll << 21)) b = 21;
+                else while ((1ll << b) < m) ++b;
+                bits += b;
+            }
+            local_bits = std::max(local_bits, bits);
+        }
+        if (!W.brute || !W.fbrute) {
             w->any_grid = 1;
             if (!p.periodic) all_periodic = false;
             int bits = 0;
@@ -300,6 +356,10 @@ int derive_worlds(NeWorld* w, const std::vector<uint32_t>& planes) {
     int rc;
     if ((rc = dalloc(&w->d_wp, nw)) || (rc = dalloc(&w->d_cext, 6 * (size_t)nw))) return rc;
     NE_CUDA_TRY(cudaMemcpy(w->d_wp, w->h_wp.data(), nw * sizeof(neb::WorldP), cudaMemcpyHostToDevice));
+    dfree(w->d.xlist);
+    if ((rc = dalloc(&w->d.xlist, xlist.size() ? xlist.size() : 1))) return rc;
+    if (!xlist.empty())
+        NE_CUDA_TRY(cudaMemcpy(w->d.xlist, xlist.data(), xlist.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     return NE_OK;
 }
 
@@ -376,7 +436,7 @@ int ne_world_destroy(NeWorld* w) {
     dfree(d.verts); dfree(d.nc); dfree(d.planes);
     for (int b = 0; b < 2; ++b) { dfree(d.wkey[b]); dfree(d.wimp[b]); }
     dfree(d.hist); dfree(d.tsum); dfree(d.ctl);
-    dfree(w->d_wp); dfree(w->d_bw); dfree(w->d_cext);
+    dfree(w->d_wp); dfree(w->d_bw); dfree(w->d_cext); dfree(d.xlist); dfree(d.rec_i); dfree(d.rec_j);
     if (w->h_ctl) cudaFreeHost(w->h_ctl);
     if (w->pinned) cudaFreeHost(w->pinned);
     for (int k = 0; k <= NE_NUM_STAGES; ++k)
@@ -513,6 +573,23 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
         st[i] = neb::D4{b->friction[i], b->restitution[i], b->linear_damping[i], b->angular_damping[i]};
     if ((rc = put(d.mat))) return rc;
 
+    // Large bodies: bounding radius above 4x the world's 90th-percentile
+    // radius, unless that would flag more than 5% of the world (then none).
+    w->h_large.assign(n ? n : 1, 0);
+    for (uint32_t k = 0; k < nworlds; ++k) {
+        std::vector<double> r;
+        for (uint32_t i = wbegin[k]; i < wbegin[k + 1]; ++i)
+            if (shapes[i] != NE_SHAPE_PLANE && shapes[i] != NE_SHAPE_MESH) r.push_back(boundR[i]);
+        if (r.size() < 8) continue;
+        std::vector<double> sr = r;
+        std::sort(sr.begin(), sr.end());
+        const double split = 4.0 * sr[(size_t)(0.9 * (double)(sr.size() - 1))];
+        size_t nlarge = 0;
+        for (double x : r) nlarge += x > split;
+        if (nlarge == 0 || nlarge > std::max<size_t>(4, r.size() / 20)) continue;
+        for (uint32_t i = wbegin[k]; i < wbegin[k + 1]; ++i)
+            if (shapes[i] != NE_SHAPE_PLANE && shapes[i] != NE_SHAPE_MESH && boundR[i] > split) w->h_large[i] = 1;
+    }
     std::vector<uint4> meta(n ? n : 1);
     std::vector<uint2> vr(n ? n : 1), ncr(n ? n : 1);
     for (uint32_t i = 0; i < n; ++i) {
@@ -520,6 +597,7 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
         const bool mut = b->inv_mass[i] > 0.0 || b->inv_inertia[3 * i] != 0.0 || b->inv_inertia[3 * i + 1] != 0.0 ||
                          b->inv_inertia[3 * i + 2] != 0.0;
         if (mut) fl |= neb::kFlagMutable;
+        if (w->h_large[i]) fl |= neb::kFlagLarge;
         meta[i] = make_uint4((uint32_t)b->shape[i], fl, b->layer[i], b->mask[i]);
         vr[i] = (b->shape[i] == NE_SHAPE_CONVEX) ? make_uint2(b->vert_offset[i], b->vert_count[i]) : make_uint2(0, 0);
         ncr[i] = (b->nocollide_count && b->nocollide_count[i])
@@ -555,9 +633,11 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
 
     // Initial capacities; they grow on demand (see ne_world_step).
     if (!w->Pcap) {
-        if ((rc = alloc_pairs(w, std::max<uint64_t>(16ull * n, 4096)))) return rc;
-        if ((rc = alloc_surv(w, std::max<uint64_t>(4ull * n, 1024)))) return rc;
-        if ((rc = alloc_cons(w, std::max<uint64_t>(4ull * n, 1024)))) return rc;
+        // Typical contact-rich scenes: ~60 grid candidates, ~4 surviving pairs
+        // and ~5 contacts per body; larger needs grow (a re-run step).
+        if ((rc = alloc_pairs(w, std::max<uint64_t>(64ull * n, 4096)))) return rc;
+        if ((rc = alloc_surv(w, std::max<uint64_t>(6ull * n, 1024)))) return rc;
+        if ((rc = alloc_cons(w, std::max<uint64_t>(8ull * n, 1024)))) return rc;
     }
     if ((rc = alloc_scratch(w))) return rc;
     w->has_bodies = true;
@@ -690,7 +770,11 @@ int ne_world_step(NeWorld* w, uint32_t nsteps) {
                 w->key_bits = (((int)c.need_bits + 7) / 8) * 8;
                 grew = true;
             }
-            if (c.P > w->Pcap) {
+            if (c.P_ref > w->Rcap && (w->record & NE_RECORD_PAIRS)) {
+                if (c.P_ref > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 recorded pairs");
+                if ((rc = alloc_rec(w, grow_to(c.P_ref)))) return rc;
+                grew = true;
+            } else if (c.P > w->Pcap) {
                 if (c.P > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 candidate pairs");
                 if ((rc = alloc_pairs(w, grow_to(c.P)))) return rc;
                 grew = true;
@@ -720,7 +804,8 @@ int ne_world_step(NeWorld* w, uint32_t nsteps) {
             int kb = (((int)c.need_bits + 7) / 8) * 8;
             if (kb >= 8) w->key_bits = kb;
         }
-        w->stats.pairs = c.P;
+        w->stats.pairs = (w->record & NE_RECORD_PAIRS) ? c.P_ref : c.P;
+        w->stats.candidates = c.P;
         w->stats.survivors = c.S;
         w->stats.contacts = c.C;
         w->stats.islands = c.islands;
@@ -751,11 +836,13 @@ int ne_world_stats(const NeWorld* w, NeStepStats* out) {
 int ne_world_pairs(NeWorld* w, uint32_t* pi, uint32_t* pj, uint64_t cap, uint64_t* count) {
     if (!w || !count) return set_err(NE_ERR_ARG, "NULL argument");
     NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    if (!(w->record & NE_RECORD_PAIRS))
+        return set_err(NE_ERR_ARG, "pair recording is off (ne_world_set_record(world, NE_RECORD_PAIRS))");
     const uint64_t P = w->stats.pairs;
     *count = P;
     const uint64_t m = std::min(P, cap);
-    if (m && pi) NE_CUDA_TRY(cudaMemcpy(pi, w->d.pair_i, m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-    if (m && pj) NE_CUDA_TRY(cudaMemcpy(pj, w->d.pair_j, m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (m && pi) NE_CUDA_TRY(cudaMemcpy(pi, w->d.rec_i, m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (m && pj) NE_CUDA_TRY(cudaMemcpy(pj, w->d.rec_j, m * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     return NE_OK;
 }
 
@@ -803,6 +890,16 @@ int ne_world_islands(NeWorld* w, uint32_t* label, uint32_t n) {
         uint32_t x = i;
         for (uint32_t guard = 0; parent[x] != x && guard < w->n; ++guard) x = parent[x];
         label[i] = x;
+    }
+    return NE_OK;
+}
+
+int ne_world_set_record(NeWorld* w, uint32_t flags) {
+    if (!w) return set_err(NE_ERR_ARG, "world is NULL");
+    w->record = flags;
+    if ((flags & NE_RECORD_PAIRS) && !w->d.rec_i) {
+        int rc = alloc_rec(w, std::max<uint64_t>(16ull * w->n, 4096));
+        if (rc) return rc;
     }
     return NE_OK;
 }

@@ -29,6 +29,10 @@ namespace neb {
 // Internal body flag: the solver can change this body's velocity
 // (invMass > 0 or a nonzero inverse inertia).  Immovable bodies separate islands.
 constexpr uint32_t kFlagMutable = 1u << 16;
+// Internal body flag: bounding radius far above its world's typical size (a
+// ground box, a wall).  The internal grid pairs such bodies with every body of
+// the world, like planes, so they do not set the cell size.
+constexpr uint32_t kFlagLarge = 1u << 17;
 
 // Device control block: capacity checks, counters, warm-cache selector.
 struct Ctl {
@@ -37,7 +41,8 @@ struct Ctl {
     uint32_t need_bits;      // sort-key bits the cell keys needed
     uint32_t local_bits;     // widest per-world cell-key layout this step
     uint32_t wsel;           // warm cache buffer holding the previous step
-    uint64_t P, S, C;        // pairs, survivors, contacts (totals, even if over capacity)
+    uint64_t P, S, C;        // candidate pairs, survivors, contacts (totals, even if over capacity)
+    uint64_t P_ref;          // pairs of the reference's broadphase rule (recorded steps)
     uint64_t islands, max_island, epa_cap_hits;
     uint32_t nbig;           // islands solved by the dataflow kernel this step
     uint32_t solve_timeout;  // a bounded dependency wait ran out (error)
@@ -54,14 +59,16 @@ struct DevWorld {
     D4* verts;
     uint2* ncrng;
     uint32_t* nc;
-    uint32_t* planes;        // indices of grid-excluded bodies, ascending
+    uint32_t* planes;        // indices of grid-excluded bodies (planes), ascending
+    uint32_t* xlist;         // planes and large bodies, ascending (internal grid)
     // pre-step snapshot (restored when a step is re-run)
     D4 *s_pos, *s_quat, *s_vel, *s_omg, *s_frc, *s_trq;
     // broadphase
     unsigned long long *key[2];
     uint32_t* val[2];
     uint32_t *bcnt, *boff;
-    uint32_t *pair_i, *pair_j;
+    uint32_t *pair_i, *pair_j;     // internal candidate pairs (CSR by first body)
+    uint32_t *rec_i, *rec_j;       // reference-rule pair list (recorded steps only)
     // narrowphase
     uint32_t *pflag, *poff, *surv;
     uint32_t *ccnt, *coff;

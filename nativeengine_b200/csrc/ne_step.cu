@@ -49,14 +49,49 @@ __device__ __forceinline__ BodyG load_geom(const DevWorld& d, uint32_t i) {
 
 __device__ __forceinline__ int bitlen_u64(unsigned long long x) { return x ? 64 - __clzll((long long)x) : 0; }
 
-// Per-axis cell coordinate (src/world.cpp:458-466), in world W's grid.
-__device__ __forceinline__ long long cell_of(const WorldP& W, double c, int axis) {
+// Grid used by one broadphase pass: the reference's (cell = 2 * max bounding
+// radius, planes excluded) or the internal one (large bodies excluded like
+// planes, cell from the remaining bodies).
+struct GridSel {
+    double cell;
+    long long nc[3];
+    int brute;
+    const uint32_t* xl;      // excluded bodies of the world, ascending
+    uint32_t xb, xe;
+};
+
+__device__ __forceinline__ GridSel grid_sel(const StepArgs& a, const WorldP& W, int fast) {
+    GridSel G;
+    if (fast) {
+        G.cell = W.fcell;
+        for (int k = 0; k < 3; ++k) G.nc[k] = W.fnc[k];
+        G.brute = W.fbrute;
+        G.xl = a.d.xlist;
+        G.xb = W.xl_begin;
+        G.xe = W.xl_end;
+    } else {
+        G.cell = W.cell;
+        for (int k = 0; k < 3; ++k) G.nc[k] = W.nc[k];
+        G.brute = W.brute;
+        G.xl = a.d.planes;
+        G.xb = W.plane_begin;
+        G.xe = W.plane_end;
+    }
+    return G;
+}
+
+__device__ __forceinline__ bool excluded(uint4 m, int fast) {
+    return grid_excluded((int)m.x) || (fast && (m.y & kFlagLarge));
+}
+
+// Per-axis cell coordinate (src/world.cpp:458-466), in grid G of world W.
+__device__ __forceinline__ long long cell_of(const WorldP& W, const GridSel& G, double c, int axis) {
     if (W.dom.periodic) {
-        long long k = (long long)floor((c + W.dom.half) / W.cell);
-        long long m = W.nc[axis];
+        long long k = (long long)floor((c + W.dom.half) / G.cell);
+        long long m = G.nc[axis];
         return ((k % m) + m) % m;
     }
-    return (long long)floor(c / W.cell);
+    return (long long)floor(c / G.cell);
 }
 
 // Compact sort key layout: a bijection of the reference's 21-bit-masked cell
@@ -72,11 +107,11 @@ struct KeyLayout {
     unsigned long long prefix;
 };
 
-__device__ __forceinline__ KeyLayout world_layout(const WorldP& W, const long long* ext) {
+__device__ __forceinline__ KeyLayout world_layout(const WorldP& W, const GridSel& G, const long long* ext) {
     KeyLayout L;
     for (int ax = 0; ax < 3; ++ax) {
         if (W.dom.periodic) {
-            const long long m = W.nc[ax];
+            const long long m = G.nc[ax];
             L.bits[ax] = (m > (1ll << 21)) ? 21 : bitlen_u64((unsigned long long)(m - 1));
             L.base[ax] = 0;
             L.span[ax] = m - 1;
@@ -94,8 +129,8 @@ __device__ __forceinline__ KeyLayout world_layout(const WorldP& W, const long lo
 
 // Layout of world w's keys; local keys of every world use the low
 // `local_bits` bits (the widest world's total).
-__device__ __forceinline__ KeyLayout key_layout(const StepArgs& a, uint32_t w, int local_bits) {
-    KeyLayout L = world_layout(a.wp[w], a.cext + 6 * (size_t)w);
+__device__ __forceinline__ KeyLayout key_layout(const StepArgs& a, uint32_t w, const GridSel& G, int local_bits) {
+    KeyLayout L = world_layout(a.wp[w], G, a.cext + 6 * (size_t)w);
     L.prefix = (unsigned long long)w << local_bits;
     return L;
 }
@@ -127,21 +162,21 @@ __device__ __forceinline__ unsigned long long neighbour_key(const KeyLayout& L, 
     return compact_key(L, cx, cy, cz);
 }
 
-__device__ __forceinline__ long long wrap_cell(const WorldP& W, long long c, int axis) {
+__device__ __forceinline__ long long wrap_cell(const WorldP& W, const GridSel& G, long long c, int axis) {
     if (!W.dom.periodic) return c;
-    const long long m = W.nc[axis];
+    const long long m = G.nc[axis];
     return ((c % m) + m) % m;
 }
 
 // The distinct neighbour keys of a cell (27 offsets; wrapping can alias them).
-__device__ __forceinline__ int neighbour_keys(const WorldP& W, const KeyLayout& L, long long cx, long long cy,
-                                              long long cz, unsigned long long* out) {
+__device__ __forceinline__ int neighbour_keys(const WorldP& W, const GridSel& G, const KeyLayout& L, long long cx,
+                                              long long cy, long long cz, unsigned long long* out) {
     int nk = 0;
     for (int dx = -1; dx <= 1; ++dx)
         for (int dy = -1; dy <= 1; ++dy)
             for (int dz = -1; dz <= 1; ++dz) {
-                unsigned long long k = neighbour_key(L, wrap_cell(W, cx + dx, 0), wrap_cell(W, cy + dy, 1),
-                                                     wrap_cell(W, cz + dz, 2));
+                unsigned long long k = neighbour_key(L, wrap_cell(W, G, cx + dx, 0), wrap_cell(W, G, cy + dy, 1),
+                                                     wrap_cell(W, G, cz + dz, 2));
                 bool dup = false;
                 for (int t = 0; t < nk; ++t) dup |= (out[t] == k);
                 if (!dup) out[nk++] = k;
@@ -182,26 +217,17 @@ __device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t* a, uint32_t 
 
 // ---------------------------------------------------------------------------
 
-__global__ void k_step_begin(Ctl* ctl, long long* ext, uint32_t nworlds) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t == 0) {
-        ctl->abort = 0;
-        ctl->flags = 0;
-        ctl->need_bits = 0;
-        ctl->local_bits = 0;
-        ctl->P = ctl->S = ctl->C = 0;
-        ctl->islands = 0;
-        ctl->max_island = 0;
-        ctl->epa_cap_hits = 0;
-        ctl->nbig = 0;
-        ctl->solve_timeout = 0;
-    }
-    if (t < nworlds) {
-        for (int a = 0; a < 3; ++a) {
-            ext[6 * (size_t)t + a] = 0x7fffffffffffffffll;
-            ext[6 * (size_t)t + 3 + a] = (long long)0x8000000000000000ull;
-        }
-    }
+__global__ void k_step_begin(Ctl* ctl) {
+    ctl->abort = 0;
+    ctl->flags = 0;
+    ctl->need_bits = 0;
+    ctl->P = ctl->S = ctl->C = 0;
+    ctl->P_ref = 0;
+    ctl->islands = 0;
+    ctl->max_island = 0;
+    ctl->epa_cap_hits = 0;
+    ctl->nbig = 0;
+    ctl->solve_timeout = 0;
 }
 
 __device__ __forceinline__ long long warp_min_ll(long long v) {
@@ -219,9 +245,59 @@ __device__ __forceinline__ long long warp_max_ll(long long v) {
     return v;
 }
 
-// World::integrate() (src/world.cpp:373-411) + pre-step snapshot + union-find
-// reset + cell extents of the post-integration positions (per world).
+// World::integrate() (src/world.cpp:373-411) + pre-step snapshot + union-find reset.
 __global__ void __launch_bounds__(kT) k_integrate(StepArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const DevWorld& d = a.d;
+    const WorldP& W = a.wp[a.bw[i]];
+    D4 p = d.pos[i], q4 = d.quat[i], v4 = d.vel[i], w4 = d.omg[i], f4 = d.frc[i], t4 = d.trq[i];
+    d.s_pos[i] = p; d.s_quat[i] = q4; d.s_vel[i] = v4; d.s_omg[i] = w4; d.s_frc[i] = f4; d.s_trq[i] = t4;
+    d.parent[i] = i;
+    const uint4 m = d.meta[i];
+    V3 x = v3of(p), v = v3of(v4), wv = v3of(w4), F = v3of(f4), T = v3of(t4);
+    Q q = qof(q4);
+    const double invM = p.w, dt = W.dt;
+    if (m.y & NE_BODY_KINEMATIC) {
+        x = x + v * dt;
+        q = integrate_orientation(q, wv, dt);
+    } else if (invM <= 0.0) {
+    } else {
+        const D4 I = d.inert[i], g = d.geom[i], mt = d.mat[i];
+        const V3 invI = v3of(I);
+        v = v + (W.g * g.z + F * invM) * dt;
+        x = x + v * dt;
+        V3 L = angular_momentum(q, invI, wv);
+        L = L + T * dt;
+        q = integrate_orientation(q, wv, dt);
+        wv = apply_inv_inertia(q, invI, L);
+        if (mt.z > 0.0) v = v * (1.0 / (1.0 + mt.z * dt));
+        if (mt.w > 0.0) wv = wv * (1.0 / (1.0 + mt.w * dt));
+    }
+    F = mk(0.0, 0.0, 0.0);
+    T = F;
+    d.pos[i] = d4of(x, invM);
+    d.quat[i] = d4ofq(q);
+    d.vel[i] = d4of(v, 0.0);
+    d.omg[i] = d4of(wv, 0.0);
+    d.frc[i] = d4of(F, 0.0);
+    d.trq[i] = d4of(T, 0.0);
+}
+
+__global__ void __launch_bounds__(kT) k_ext_reset(StepArgs a) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) a.d.ctl->local_bits = 0;
+    if (t >= a.nworlds) return;
+    for (int ax = 0; ax < 3; ++ax) {
+        a.cext[6 * (size_t)t + ax] = 0x7fffffffffffffffll;
+        a.cext[6 * (size_t)t + 3 + ax] = (long long)0x8000000000000000ull;
+    }
+}
+
+// Cell extents of each open/reflective world's grid bodies (one atomic per
+// warp when the warp's bodies share a world).
+__global__ void __launch_bounds__(kT) k_extents(StepArgs a, int fast) {
+    if (a.d.ctl->abort) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool live = i < a.n;
     const uint32_t w = live ? a.bw[i] : 0xffffffffu;
@@ -230,46 +306,15 @@ __global__ void __launch_bounds__(kT) k_integrate(StepArgs a) {
                        (long long)0x8000000000000000ull};
     bool track = false;
     if (live) {
-        const DevWorld& d = a.d;
         const WorldP& W = a.wp[w];
-        D4 p = d.pos[i], q4 = d.quat[i], v4 = d.vel[i], w4 = d.omg[i], f4 = d.frc[i], t4 = d.trq[i];
-        d.s_pos[i] = p; d.s_quat[i] = q4; d.s_vel[i] = v4; d.s_omg[i] = w4; d.s_frc[i] = f4; d.s_trq[i] = t4;
-        d.parent[i] = i;
-        const uint4 m = d.meta[i];
-        V3 x = v3of(p), v = v3of(v4), wv = v3of(w4), F = v3of(f4), T = v3of(t4);
-        Q q = qof(q4);
-        const double invM = p.w, dt = W.dt;
-        if (m.y & NE_BODY_KINEMATIC) {
-            x = x + v * dt;
-            q = integrate_orientation(q, wv, dt);
-        } else if (invM <= 0.0) {
-        } else {
-            const D4 I = d.inert[i], g = d.geom[i], mt = d.mat[i];
-            const V3 invI = v3of(I);
-            v = v + (W.g * g.z + F * invM) * dt;
-            x = x + v * dt;
-            V3 L = angular_momentum(q, invI, wv);
-            L = L + T * dt;
-            q = integrate_orientation(q, wv, dt);
-            wv = apply_inv_inertia(q, invI, L);
-            if (mt.z > 0.0) v = v * (1.0 / (1.0 + mt.z * dt));
-            if (mt.w > 0.0) wv = wv * (1.0 / (1.0 + mt.w * dt));
-        }
-        F = mk(0.0, 0.0, 0.0);
-        T = F;
-        d.pos[i] = d4of(x, invM);
-        d.quat[i] = d4ofq(q);
-        d.vel[i] = d4of(v, 0.0);
-        d.omg[i] = d4of(wv, 0.0);
-        d.frc[i] = d4of(F, 0.0);
-        d.trq[i] = d4of(T, 0.0);
-        if (!W.brute && !W.dom.periodic && !grid_excluded((int)m.x)) {
-            const double c[3] = {x.x, x.y, x.z};
-            for (int ax = 0; ax < 3; ++ax) lo[ax] = hi[ax] = cell_of(W, c[ax], ax);
+        const GridSel G = grid_sel(a, W, fast);
+        if (!G.brute && !W.dom.periodic && !excluded(a.d.meta[i], fast)) {
+            const D4 p = a.d.pos[i];
+            const double c[3] = {p.x, p.y, p.z};
+            for (int ax = 0; ax < 3; ++ax) lo[ax] = hi[ax] = cell_of(W, G, c[ax], ax);
             track = true;
         }
     }
-    // Extents: one atomic per warp when the warp's bodies share a world.
     const uint32_t w0 = __shfl_sync(0xffffffffu, w, 0);
     if (__all_sync(0xffffffffu, w == w0)) {
         if (!__any_sync(0xffffffffu, track)) return;
@@ -289,39 +334,41 @@ __global__ void __launch_bounds__(kT) k_integrate(StepArgs a) {
 }
 
 // Key bits each world's grid needs; the widest decides the local key width.
-__global__ void __launch_bounds__(kT) k_world_layout(StepArgs a) {
+__global__ void __launch_bounds__(kT) k_world_layout(StepArgs a, int fast) {
     Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= a.nworlds) return;
     const WorldP& W = a.wp[w];
-    if (W.brute) return;
-    const KeyLayout L = world_layout(W, a.cext + 6 * (size_t)w);
+    const GridSel G = grid_sel(a, W, fast);
+    if (G.brute) return;
+    const KeyLayout L = world_layout(W, G, a.cext + 6 * (size_t)w);
     atomicMax(&ctl->local_bits, (uint32_t)L.total);
 }
 
-// Sort keys of the grid cells; grid-excluded bodies and bodies of
-// brute-force worlds get a sentinel that sorts after every real key.
-__global__ void __launch_bounds__(kT) k_cell_keys(StepArgs a) {
+// Sort keys of the grid cells; excluded bodies and bodies of brute-force
+// worlds get a sentinel that sorts after every real key.
+__global__ void __launch_bounds__(kT) k_cell_keys(StepArgs a, int fast) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lb = (int)ctl->local_bits;
     const int total = a.world_bits + lb;
     if (i == 0) {
-        ctl->need_bits = (uint32_t)(total + 1);
+        ctl->need_bits = max(ctl->need_bits, (uint32_t)(total + 1));
         if (total + 1 > a.key_bits) ctl->abort = 1;
     }
     if (i >= a.n) return;
     const uint32_t w = a.bw[i];
     const WorldP& W = a.wp[w];
+    const GridSel G = grid_sel(a, W, fast);
     const D4 p = a.d.pos[i];
-    const int shape = (int)a.d.meta[i].x;
     unsigned long long k;
-    if (W.brute || grid_excluded(shape)) {
+    if (G.brute || excluded(a.d.meta[i], fast)) {
         k = 1ull << total;
     } else {
-        const KeyLayout L = key_layout(a, w, lb);
-        k = compact_key(L, cell_of(W, p.x, 0), cell_of(W, p.y, 1), cell_of(W, p.z, 2));
+        const KeyLayout L = key_layout(a, w, G, lb);
+        k = compact_key(L, cell_of(W, G, p.x, 0), cell_of(W, G, p.y, 1), cell_of(W, G, p.z, 2));
     }
     a.d.key[0][i] = k;
     a.d.val[0][i] = i;
@@ -329,7 +376,7 @@ __global__ void __launch_bounds__(kT) k_cell_keys(StepArgs a) {
 
 // Number of partners j > i of body i (the sorted unique pair list is the CSR
 // of these partner lists).  Partners are always in body i's world.
-__global__ void __launch_bounds__(kT) k_pair_count(StepArgs a, int kb) {
+__global__ void __launch_bounds__(kT) k_pair_count(StepArgs a, int kb, int fast) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -337,14 +384,15 @@ __global__ void __launch_bounds__(kT) k_pair_count(StepArgs a, int kb) {
     const DevWorld& d = a.d;
     const uint32_t w = a.bw[i];
     const WorldP& W = a.wp[w];
-    if (W.brute || grid_excluded((int)d.meta[i].x)) {
+    const GridSel G = grid_sel(a, W, fast);
+    if (G.brute || excluded(d.meta[i], fast)) {
         d.bcnt[i] = W.end - 1 - i;
         return;
     }
-    const KeyLayout L = key_layout(a, w, (int)ctl->local_bits);
+    const KeyLayout L = key_layout(a, w, G, (int)ctl->local_bits);
     const D4 p = d.pos[i];
     unsigned long long nk[27];
-    const int m = neighbour_keys(W, L, cell_of(W, p.x, 0), cell_of(W, p.y, 1), cell_of(W, p.z, 2), nk);
+    const int m = neighbour_keys(W, G, L, cell_of(W, G, p.x, 0), cell_of(W, G, p.y, 1), cell_of(W, G, p.z, 2), nk);
     const unsigned long long* keys = d.key[kb];
     const uint32_t* vals = d.val[kb];
     uint32_t cnt = 0;
@@ -355,20 +403,21 @@ __global__ void __launch_bounds__(kT) k_pair_count(StepArgs a, int kb) {
         uint32_t s = upper_bound_u32(vals, lo, hi, i);
         cnt += hi - s;
     }
-    cnt += W.plane_end - upper_bound_u32(d.planes, W.plane_begin, W.plane_end, i);
+    cnt += G.xe - upper_bound_u32(G.xl, G.xb, G.xe, i);
     d.bcnt[i] = cnt;
 }
 
 // Writes body i's sorted partner list at its CSR offset.  One warp per body.
 // The partner candidates are up to 27 sorted runs (one per distinct
 // neighbour cell; members with index > i) plus the sorted run of the world's
-// planes > i.  Lanes split the concatenated candidates evenly; each
+// excluded bodies > i.  Lanes split the concatenated candidates evenly; each
 // candidate's output rank is its index in its own run plus the number of
 // smaller candidates in the other runs (all candidates are distinct bodies).
-__global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
+__global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb, int fast, uint32_t* out_i, uint32_t* out_j,
+                                                  const uint64_t* total_p, uint64_t cap) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
-    if (ctl->P > a.Pcap) {
+    if (*total_p > cap) {
         if (threadIdx.x == 0 && blockIdx.x == 0) ctl->abort = 1;
         return;
     }
@@ -379,27 +428,28 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
     const DevWorld& d = a.d;
     const uint32_t w = a.bw[i];
     const WorldP& W = a.wp[w];
+    const GridSel G = grid_sel(a, W, fast);
     const uint32_t base = d.boff[i];
-    if (W.brute || grid_excluded((int)d.meta[i].x)) {
+    if (G.brute || excluded(d.meta[i], fast)) {
         const uint32_t cnt = W.end - 1 - i;
         for (uint32_t k = lane; k < cnt; k += 32) {
-            d.pair_i[base + k] = i;
-            d.pair_j[base + k] = i + 1 + k;
+            out_i[base + k] = i;
+            out_j[base + k] = i + 1 + k;
         }
         return;
     }
-    const KeyLayout L = key_layout(a, w, (int)ctl->local_bits);
+    const KeyLayout L = key_layout(a, w, G, (int)ctl->local_bits);
     const D4 p = d.pos[i];
-    const long long cx = cell_of(W, p.x, 0), cy = cell_of(W, p.y, 1), cz = cell_of(W, p.z, 2);
+    const long long cx = cell_of(W, G, p.x, 0), cy = cell_of(W, G, p.y, 1), cz = cell_of(W, G, p.z, 2);
     const unsigned long long* keys = d.key[kb];
     const uint32_t* vals = d.val[kb];
     // Lane t < 27 takes neighbour offset t (duplicates from wrap aliasing keep
-    // their lowest lane); lane 27 takes the plane list.
+    // their lowest lane); lane 27 takes the excluded list.
     uint32_t rlo = 0, rhi = 0;
     if (lane < 27) {
         const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
-        unsigned long long k = neighbour_key(L, wrap_cell(W, cx + dx, 0), wrap_cell(W, cy + dy, 1),
-                                             wrap_cell(W, cz + dz, 2));
+        unsigned long long k = neighbour_key(L, wrap_cell(W, G, cx + dx, 0), wrap_cell(W, G, cy + dy, 1),
+                                             wrap_cell(W, G, cz + dz, 2));
         const uint32_t grp = __match_any_sync(0x07ffffffu, k);
         if (lane == __ffs(grp) - 1) {
             uint32_t lo = lower_bound_u64(keys, 0, a.n, k);
@@ -408,8 +458,8 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
             rhi = hi;
         }
     } else if (lane == 27) {
-        rlo = upper_bound_u32(d.planes, W.plane_begin, W.plane_end, i);
-        rhi = W.plane_end;
+        rlo = upper_bound_u32(G.xl, G.xb, G.xe, i);
+        rhi = G.xe;
     }
     // Compact the non-empty runs into shared memory, in lane order.
     const uint32_t len = rhi - rlo;
@@ -422,8 +472,8 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
     }
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     const int nr = __popc(nonempty);
-    // The plane run (lane 27) is the last non-empty run if present.
-    const bool planes_nonempty = (nonempty >> 27) & 1u;
+    // The excluded run (lane 27) is the last non-empty run if present.
+    const bool xl_nonempty = (nonempty >> 27) & 1u;
     if (len > 0) {
         s_lo[wid][r] = rlo;
         s_len[wid][r] = len;
@@ -440,17 +490,17 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb) {
         }
         const int own = lo;
         const uint32_t idx = e - s_ex[wid][own];
-        const bool own_plane = planes_nonempty && own == nr - 1;
-        const uint32_t x = own_plane ? d.planes[s_lo[wid][own] + idx] : vals[s_lo[wid][own] + idx];
+        const bool own_xl = xl_nonempty && own == nr - 1;
+        const uint32_t x = own_xl ? G.xl[s_lo[wid][own] + idx] : vals[s_lo[wid][own] + idx];
         uint32_t rank = idx;
         for (int q = 0; q < nr; ++q) {
             if (q == own) continue;
             const uint32_t ql = s_lo[wid][q], qh = ql + s_len[wid][q];
-            const uint32_t* src = (planes_nonempty && q == nr - 1) ? d.planes : vals;
+            const uint32_t* src = (xl_nonempty && q == nr - 1) ? G.xl : vals;
             rank += lower_bound_u32(src, ql, qh, x) - ql;
         }
-        d.pair_i[base + rank] = i;
-        d.pair_j[base + rank] = x;
+        out_i[base + rank] = i;
+        out_j[base + rank] = x;
     }
 }
 
@@ -1110,22 +1160,31 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
         if (ev) cudaEventRecord(ev[k], st);
     };
     mark(0);
-    k_step_begin<<<blocks_for(a.nworlds, kT), kT, 0, st>>>(ctl, a.cext, a.nworlds); ++L;
+    k_step_begin<<<1, 1, 0, st>>>(ctl); ++L;
     k_integrate<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
 
     mark(1);
     // Broadphase: cell keys -> stable sort -> per-body partner counts -> CSR.
-    int kb = 0;
-    if (a.any_grid) {
-        k_world_layout<<<blocks_for(a.nworlds, kT), kT, 0, st>>>(a); ++L;
-        k_cell_keys<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
-        unsigned long long* keys[2] = {d.key[0], d.key[1]};
-        uint32_t* vals[2] = {d.val[0], d.val[1]};
-        kb = radix_sort_u64(keys, vals, a.n, a.key_bits, d.hist, d.tsum, ctl, st, launches);
+    // Pass 0 (recorded steps only) builds the reference-rule pair list; pass 1
+    // builds the internal candidate list the cull consumes.
+    for (int fast = a.record ? 0 : 1; fast <= 1; ++fast) {
+        int kb = 0;
+        if (a.any_grid) {
+            k_ext_reset<<<blocks_for(a.nworlds, kT), kT, 0, st>>>(a); ++L;
+            k_extents<<<blocks_for(a.n, kT), kT, 0, st>>>(a, fast); ++L;
+            k_world_layout<<<blocks_for(a.nworlds, kT), kT, 0, st>>>(a, fast); ++L;
+            k_cell_keys<<<blocks_for(a.n, kT), kT, 0, st>>>(a, fast); ++L;
+            unsigned long long* keys[2] = {d.key[0], d.key[1]};
+            uint32_t* vals[2] = {d.val[0], d.val[1]};
+            kb = radix_sort_u64(keys, vals, a.n, a.key_bits, d.hist, d.tsum, ctl, st, launches);
+        }
+        k_pair_count<<<blocks_for(a.n, kT), kT, 0, st>>>(a, kb, fast); ++L;
+        uint64_t* total = fast ? &ctl->P : &ctl->P_ref;
+        scan_u32(d.bcnt, d.boff, a.n, d.tsum, total, ctl, st, launches);
+        k_pair_emit<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a, kb, fast, fast ? d.pair_i : d.rec_i,
+                                                                      fast ? d.pair_j : d.rec_j, total,
+                                                                      fast ? a.Pcap : a.Rcap); ++L;
     }
-    k_pair_count<<<blocks_for(a.n, kT), kT, 0, st>>>(a, kb); ++L;
-    scan_u32(d.bcnt, d.boff, a.n, d.tsum, &ctl->P, ctl, st, launches);
-    k_pair_emit<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a, kb); ++L;
 
     mark(2);
     // Narrowphase on the pairs that survive the filters and the cull.

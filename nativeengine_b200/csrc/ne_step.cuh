@@ -21,8 +21,14 @@ struct WorldP {
     int brute;               // forceBruteForce || n < 64 || cell < 1e-9
     double cell;             // 2 * max bounding radius
     long long nc[3];         // periodic cell counts
+    // internal grid: large bodies excluded like planes; the cell bounds every
+    // pair the cull can keep (see derive_worlds in ne_capi.cu)
+    int fbrute;
+    double fcell;
+    long long fnc[3];
     uint32_t begin, end;     // body range
-    uint32_t plane_begin, plane_end;   // range of this world's grid-excluded bodies in DevWorld::planes
+    uint32_t plane_begin, plane_end;   // range of this world's planes in DevWorld::planes
+    uint32_t xl_begin, xl_end;         // range of this world's planes + large bodies in DevWorld::xlist
 };
 
 struct StepArgs {
@@ -36,7 +42,8 @@ struct StepArgs {
     int key_bits;            // bits the cell-key sort covers this step
     int any_grid;            // some world uses the grid (else every world is brute force)
     int warm;                // warm starting (one setting for the whole batch)
-    uint64_t Pcap, Scap, Ccap;
+    int record;              // also build the reference-rule pair list
+    uint64_t Pcap, Scap, Ccap, Rcap;
     int num_sms;
 };
 

@@ -20,13 +20,18 @@ def _ptr(a: Optional[np.ndarray]):
 
 
 class DeviceWorld:
-    def __init__(self, params: Optional[_ffi.NeWorldParams] = None, bodies: Optional[BodyArrays] = None):
+    def __init__(self, params: Optional[_ffi.NeWorldParams] = None, bodies: Optional[BodyArrays] = None,
+                 record: bool = True):
+        """record=True keeps the reference-rule pair list of every step for
+        pairs() (the parity tests need it); benchmarks pass record=False."""
         self._lib = _ffi.load()
         self.params = params if params is not None else default_params()
         h = C.c_void_p()
         _ffi.check(self._lib.ne_world_create(C.byref(self.params), C.byref(h)), "ne_world_create")
         self._h = h
         self.n = 0
+        if record:
+            _ffi.check(self._lib.ne_world_set_record(self._h, _ffi.RECORD_PAIRS), "ne_world_set_record")
         if bodies is not None:
             self.upload(bodies)
 
