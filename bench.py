@@ -100,6 +100,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="box_pile",
                     help="workload (box_pile is the headline; the others are for profiling and extra lines)")
+    ap.add_argument("--precision", choices=("f64", "f32"), default="f64",
+                    help="f64: bit-exact with the reference; f32: the batched FP32 form")
+    ap.add_argument("--autotune", action="store_true", help="tune the big-island solver shape before timing")
     return ap.parse_args()
 
 
@@ -296,15 +299,16 @@ def run_ours(args):
     begin = made[2] if len(made) > 2 else None
     n = bodies.n
     if begin is None:
-        dev = DeviceWorld(params, bodies.copy(), record=False)
+        dev = DeviceWorld(params, bodies.copy(), record=False, precision=args.precision)
     else:
-        dev = DeviceWorld(params[0], None, record=False)
+        dev = DeviceWorld(params[0], None, record=False, precision=args.precision)
         dev.upload_batch(params, bodies.copy(), begin)
     stream = torch.cuda.ExternalStream(dev.stream_handle())
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
 
     # Warm-up: W steps from the initial state (grows the device buffers).
     dev.step(max(args.warmup, 0))
+    shape = dev.autotune(steps=3) if args.autotune else dev.solver_shape()
 
     def barrier():
         torch.cuda.synchronize()
@@ -380,8 +384,11 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
             "ms_per_step": t_dev / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload, "bodies": n, "steps_per_run": K,
+            "dtype": "f64" if args.precision == "f64" else "f32 (FP64 poses, wrap, warm impulses, EPA tests)",
+            "data": "synthetic",
+            "config": {"workload": workload, "bodies": n, "steps_per_run": K, "precision": args.precision,
+                       "solver_shape": {"threads": shape[0], "ctas_per_sm": shape[1],
+                                        "autotuned": bool(args.autotune)},
                        "parallelism": "replicas" if world > 1 else "single world",
                        "l2": "256 MiB buffer rewritten between timed steps (outside the events)"},
             "roofline": {"bound": "hbm", "kernel": "solve (k_island_solve + k_island_solve_big)",

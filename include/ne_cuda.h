@@ -230,6 +230,47 @@ int ne_world_contacts(NeWorld* world, NeContactArrays* out, uint64_t cap,
  * bodies in no such contact are their own label. */
 int ne_world_islands(NeWorld* world, uint32_t* label, uint32_t n);
 
+/* Arithmetic precision of the narrowphase and the contact solve.  No
+ * counterpart in the reference (which is FP64 throughout).
+ *   NE_PRECISION_F64  the default: bit-exact with the reference.
+ *   NE_PRECISION_F32  the batched FP32 form: support mappings, GJK, analytic
+ *     pairs, box-box clipping and the sequential-impulse solve in FP32 with
+ *     FP32 accumulation, in the reference's contact order; FP64 stays for
+ *     pose integration, the minimum-image offsets and the wrap, the
+ *     accumulated normal impulses (the warm-start cache), EPA's polytope and
+ *     its termination tests, and the body state between steps.
+ * Takes effect from the next step; may be changed at any time. */
+#define NE_PRECISION_F64 0
+#define NE_PRECISION_F32 1
+int ne_world_set_precision(NeWorld* world, int precision);
+
+/* Launch shape of the big-island solver (islands of >= 48 contacts, one CTA
+ * per island at a time).  No counterpart in the reference.  Results do not
+ * depend on it.  threads: 128, 256 or 512; ctas_per_sm: 1..4.
+ * ne_world_autotune times each candidate shape for `steps` steps from the
+ * current state, keeps the fastest and restores the state and warm cache, so
+ * the world continues as if it had not been called; *chosen (may be NULL)
+ * receives the shape kept. */
+typedef struct NeSolverShape {
+    uint32_t threads;
+    uint32_t ctas_per_sm;
+} NeSolverShape;
+int ne_world_set_solver_shape(NeWorld* world, const NeSolverShape* shape);
+int ne_world_get_solver_shape(const NeWorld* world, NeSolverShape* shape);
+int ne_world_autotune(NeWorld* world, uint32_t steps, NeSolverShape* chosen);
+
+/* Device checkpoint of everything a step changes: positions, orientations,
+ * velocities, angular velocities, pending forces and torques, and the warm
+ * cache (last step's accumulated normal impulses).  The device analogue of
+ * PhysicsWorld::saveState()/loadState() (src/physics_world.cpp:22-64) kept in
+ * HBM; restoring makes the next steps bit-identical to the steps taken after
+ * the checkpoint was made.  A checkpoint belongs to the world that made it
+ * and must be destroyed before that world. */
+typedef struct NeCheckpoint NeCheckpoint;
+int ne_world_checkpoint(NeWorld* world, NeCheckpoint** out);
+int ne_world_restore(NeWorld* world, const NeCheckpoint* checkpoint);
+int ne_checkpoint_destroy(NeCheckpoint* checkpoint);
+
 /* The CUDA stream the world launches on (as a void*; cast to cudaStream_t). */
 int ne_world_stream(const NeWorld* world, void** stream);
 /* Number of kernel launches made by the last ne_world_step call. */

@@ -24,6 +24,8 @@ NE_ERR_NUMERIC = 6
 NE_ERR_NO_DEVICE = 7
 NUM_STAGES = 8
 RECORD_PAIRS = 1
+PRECISION_F64 = 0
+PRECISION_F32 = 1
 NOALLOC_MAX_BODIES = 2048
 NOALLOC_MAX_PAIRS = 262144
 
@@ -86,6 +88,10 @@ class NeContactArrays(C.Structure):
     ]
 
 
+class NeSolverShape(C.Structure):
+    _fields_ = [("threads", C.c_uint32), ("ctas_per_sm", C.c_uint32)]
+
+
 class NeStepStats(C.Structure):
     _fields_ = [
         ("pairs", C.c_uint64), ("survivors", C.c_uint64), ("contacts", C.c_uint64),
@@ -114,6 +120,13 @@ EXPORTS = {
     "ne_world_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "ne_world_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
     "ne_world_set_record": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "ne_world_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "ne_world_set_solver_shape": (C.c_int, [C.c_void_p, C.POINTER(NeSolverShape)]),
+    "ne_world_get_solver_shape": (C.c_int, [C.c_void_p, C.POINTER(NeSolverShape)]),
+    "ne_world_autotune": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(NeSolverShape)]),
+    "ne_world_checkpoint": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "ne_world_restore": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ne_checkpoint_destroy": (C.c_int, [C.c_void_p]),
     "ne_world_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "ne_world_stage_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "ne_stage_name": (C.c_char_p, [C.c_int]),

@@ -2,7 +2,10 @@
 
 FP64 parity with the x86-64 reference needs ``--fmad=false`` (no fused
 multiply-add contraction); division and square root stay IEEE-rounded
-(nvcc's defaults -prec-div=true -prec-sqrt=true).
+(nvcc's defaults -prec-div=true -prec-sqrt=true).  The batched FP32 form's
+translation unit (ne_step_f32.cu) has no parity contract and is compiled with
+contraction enabled.  Each source compiles to its own object (in parallel),
+then nvcc links the shared library.
 """
 from __future__ import annotations
 
@@ -14,9 +17,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib", "libne_cuda.so")
-SOURCES = ["ne_prims.cu", "ne_step.cu", "ne_capi.cu", "ne_noalloc.cu"]
+OBJDIR = os.path.join(HERE, "_build")
+SOURCES = ["ne_prims.cu", "ne_step.cu", "ne_step_f32.cu", "ne_capi.cu", "ne_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "--fmad=false", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
+# Per-source contraction setting: off everywhere except the FP32 form.
+FMAD = {"ne_step_f32.cu": "--fmad=true"}
 
 
 def nvcc() -> str:
@@ -54,12 +60,25 @@ def build_host(force: bool = False, verbose: bool = False) -> str:
     return HOST_OUT
 
 
+def _compile(src: str, verbose: bool) -> str:
+    obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
+    cmd = [nvcc()] + ARCH + FLAGS + [FMAD.get(src, "--fmad=false"), "-I" + os.path.join(ROOT, "include"),
+                                     "-I" + CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return obj
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "ne_cuda.h")]
     if force or _stale(OUT, deps):
+        from concurrent.futures import ThreadPoolExecutor
         os.makedirs(os.path.dirname(OUT), exist_ok=True)
-        cmd = [nvcc()] + ARCH + FLAGS + ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC, "-o", OUT]
-        cmd += [os.path.join(CSRC, s) for s in SOURCES]
+        os.makedirs(OBJDIR, exist_ok=True)
+        with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+            objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", OUT] + objs
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -79,6 +79,10 @@ struct NeWorld {
     int any_grid = 0;
     std::vector<uint8_t> h_large;         // body flagged large (internal grid)
     uint32_t record = 0;                  // NE_RECORD_* flags
+    int precision = NE_PRECISION_F64;
+    uint32_t big_threads = 512;           // big-island solver launch shape
+    uint32_t big_ctas_per_sm = 1;
+    size_t nverts = 0;                    // convex vertex pool entries on the device
     uint64_t Rcap = 0;                    // capacity of the recorded pair list
     int key_bits = 64;
     int num_sms = 148;
@@ -108,6 +112,37 @@ void free_body_arrays(NeWorld* w) {
     dfree(d.s_pos); dfree(d.s_quat); dfree(d.s_vel); dfree(d.s_omg); dfree(d.s_frc); dfree(d.s_trq);
     dfree(d.key[0]); dfree(d.key[1]); dfree(d.val[0]); dfree(d.val[1]);
     dfree(d.bcnt); dfree(d.boff); dfree(d.parent); dfree(d.bdeg); dfree(d.bstart);
+    dfree(d.f_v); dfree(d.f_w); dfree(d.f_q); dfree(d.f_I); dfree(d.f_e); dfree(d.f_verts);
+}
+
+// FP32 copies of the body state and the convex vertex pool (FP32 form only).
+int alloc_f32_bodies(NeWorld* w) {
+    neb::DevWorld& d = w->d;
+    dfree(d.f_v); dfree(d.f_w); dfree(d.f_q); dfree(d.f_I); dfree(d.f_e); dfree(d.f_verts);
+    const size_t m = w->n ? w->n : 1;
+    int rc;
+    if ((rc = dalloc(&d.f_v, m)) || (rc = dalloc(&d.f_w, m)) || (rc = dalloc(&d.f_q, m)) ||
+        (rc = dalloc(&d.f_I, m)) || (rc = dalloc(&d.f_e, m)) || (rc = dalloc(&d.f_verts, w->nverts ? w->nverts : 1)))
+        return rc;
+    neb::convert_verts_f32(d.verts, d.f_verts, (uint32_t)w->nverts, w->stream);
+    NE_CUDA_TRY(cudaGetLastError());
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    return NE_OK;
+}
+
+void free_f32_cons(NeWorld* w) {
+    neb::DevWorld& d = w->d;
+    dfree(d.f_n); dfree(d.f_ra); dfree(d.f_rb); dfree(d.f_kn);
+}
+
+int alloc_f32_cons(NeWorld* w, uint64_t cap) {
+    neb::DevWorld& d = w->d;
+    free_f32_cons(w);
+    int rc;
+    if ((rc = dalloc(&d.f_n, cap)) || (rc = dalloc(&d.f_ra, cap)) || (rc = dalloc(&d.f_rb, cap)) ||
+        (rc = dalloc(&d.f_kn, cap)))
+        return rc;
+    return NE_OK;
 }
 
 void free_pair_arrays(NeWorld* w) {
@@ -137,6 +172,7 @@ void free_con_arrays(NeWorld* w) {
     dfree(d.ioff); dfree(d.istart); dfree(d.big); dfree(d.con_kn);
     dfree(d.rkey[0]); dfree(d.rkey[1]); dfree(d.rval[0]); dfree(d.rval[1]); dfree(d.crank);
     dfree(d.bcnt10); dfree(d.bq10);
+    free_f32_cons(w);
 }
 
 int alloc_scratch(NeWorld* w) {
@@ -190,6 +226,7 @@ int alloc_cons(NeWorld* w, uint64_t cap) {
         (rc = dalloc(&d.rval[1], 2 * cap)) || (rc = dalloc(&d.crank, 2 * cap)) ||
         (rc = dalloc(&d.bcnt10, 10 * cap)) || (rc = dalloc(&d.bq10, 10 * cap)))
         return rc;
+    if (w->precision == NE_PRECISION_F32 && (rc = alloc_f32_cons(w, cap))) return rc;
     unsigned long long* nk[2] = {nullptr, nullptr};
     double* ni[2] = {nullptr, nullptr};
     for (int b = 0; b < 2; ++b) {
@@ -228,6 +265,9 @@ neb::StepArgs make_args(const NeWorld* w) {
     a.any_grid = w->any_grid;
     a.warm = w->wparams.empty() ? (w->p.warm_start ? 1 : 0) : (w->wparams[0].warm_start ? 1 : 0);
     a.record = (w->record & NE_RECORD_PAIRS) ? 1 : 0;
+    a.f32 = w->precision == NE_PRECISION_F32 ? 1 : 0;
+    a.big_threads = (int)w->big_threads;
+    a.big_ctas_per_sm = (int)w->big_ctas_per_sm;
     a.Pcap = w->Pcap;
     a.Scap = w->Scap;
     a.Ccap = w->Ccap;
@@ -550,6 +590,8 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
     dfree(d.verts);
     if ((rc = dalloc(&d.verts, verts.size()))) return rc;
     NE_CUDA_TRY(cudaMemcpy(d.verts, verts.data(), verts.size() * sizeof(neb::D4), cudaMemcpyHostToDevice));
+    w->nverts = b->n_verts;
+    if (w->precision == NE_PRECISION_F32 && (rc = alloc_f32_bodies(w))) return rc;
 
     std::vector<double> boundR(n);
     std::vector<int> shapes(n);
@@ -892,6 +934,188 @@ int ne_world_islands(NeWorld* w, uint32_t* label, uint32_t n) {
         label[i] = x;
     }
     return NE_OK;
+}
+
+int ne_world_set_precision(NeWorld* w, int precision) {
+    if (!w) return set_err(NE_ERR_ARG, "world is NULL");
+    if (precision != NE_PRECISION_F64 && precision != NE_PRECISION_F32)
+        return set_err(NE_ERR_ARG, "precision must be NE_PRECISION_F64 or NE_PRECISION_F32");
+    NE_CUDA_TRY(cudaSetDevice(w->device));
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    if (precision == w->precision) return NE_OK;
+    w->precision = precision;
+    int rc;
+    if (precision == NE_PRECISION_F32) {
+        if (w->d.pos && (rc = alloc_f32_bodies(w))) return rc;
+        if (w->Ccap && (rc = alloc_f32_cons(w, w->Ccap))) return rc;
+    } else {
+        neb::DevWorld& d = w->d;
+        dfree(d.f_v); dfree(d.f_w); dfree(d.f_q); dfree(d.f_I); dfree(d.f_e); dfree(d.f_verts);
+        free_f32_cons(w);
+    }
+    return NE_OK;
+}
+
+int ne_world_set_solver_shape(NeWorld* w, const NeSolverShape* s) {
+    if (!w || !s) return set_err(NE_ERR_ARG, "NULL argument");
+    if (s->threads != 128 && s->threads != 256 && s->threads != 512)
+        return set_err(NE_ERR_ARG, "solver threads must be 128, 256 or 512");
+    if (s->ctas_per_sm < 1 || s->ctas_per_sm > 4) return set_err(NE_ERR_ARG, "solver ctas_per_sm must be 1..4");
+    w->big_threads = s->threads;
+    w->big_ctas_per_sm = s->ctas_per_sm;
+    return NE_OK;
+}
+
+int ne_world_get_solver_shape(const NeWorld* w, NeSolverShape* s) {
+    if (!w || !s) return set_err(NE_ERR_ARG, "NULL argument");
+    s->threads = w->big_threads;
+    s->ctas_per_sm = w->big_ctas_per_sm;
+    return NE_OK;
+}
+
+// Device copy of the state a step changes: the six body arrays and the warm
+// cache (the buffer holding the last step's impulses).
+struct Saved {
+    neb::D4* body[6] = {};
+    unsigned long long* wkey = nullptr;
+    double* wimp = nullptr;
+    uint32_t wsel = 0, wcount = 0;
+    NeStepStats stats{};
+};
+
+static void saved_free(Saved& s) {
+    for (auto*& p : s.body) dfree(p);
+    dfree(s.wkey);
+    dfree(s.wimp);
+}
+
+static int save_state(NeWorld* w, Saved& s) {
+    neb::DevWorld& d = w->d;
+    neb::D4* src[6] = {d.pos, d.quat, d.vel, d.omg, d.frc, d.trq};
+    const size_t m = w->n ? w->n : 1;
+    int rc;
+    for (int k = 0; k < 6; ++k) {
+        if ((rc = dalloc(&s.body[k], m))) return rc;
+        NE_CUDA_TRY(cudaMemcpy(s.body[k], src[k], m * sizeof(neb::D4), cudaMemcpyDeviceToDevice));
+    }
+    NE_CUDA_TRY(cudaMemcpy(w->h_ctl, d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost));
+    s.wsel = w->h_ctl->wsel;
+    s.wcount = w->h_ctl->wcount[s.wsel];
+    const size_t c = s.wcount ? s.wcount : 1;
+    if ((rc = dalloc(&s.wkey, c)) || (rc = dalloc(&s.wimp, c))) return rc;
+    if (s.wcount) {
+        NE_CUDA_TRY(cudaMemcpy(s.wkey, d.wkey[s.wsel], s.wcount * sizeof(unsigned long long), cudaMemcpyDeviceToDevice));
+        NE_CUDA_TRY(cudaMemcpy(s.wimp, d.wimp[s.wsel], s.wcount * sizeof(double), cudaMemcpyDeviceToDevice));
+    }
+    s.stats = w->stats;
+    return NE_OK;
+}
+
+static int restore_state(NeWorld* w, const Saved& s) {
+    neb::DevWorld& d = w->d;
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    neb::D4* dst[6] = {d.pos, d.quat, d.vel, d.omg, d.frc, d.trq};
+    const size_t m = w->n ? w->n : 1;
+    for (int k = 0; k < 6; ++k)
+        NE_CUDA_TRY(cudaMemcpy(dst[k], s.body[k], m * sizeof(neb::D4), cudaMemcpyDeviceToDevice));
+    // The warm buffers may have been reallocated (grown) meanwhile; the
+    // saved entries always fit.
+    if (s.wcount) {
+        NE_CUDA_TRY(cudaMemcpy(d.wkey[s.wsel], s.wkey, s.wcount * sizeof(unsigned long long), cudaMemcpyDeviceToDevice));
+        NE_CUDA_TRY(cudaMemcpy(d.wimp[s.wsel], s.wimp, s.wcount * sizeof(double), cudaMemcpyDeviceToDevice));
+    }
+    NE_CUDA_TRY(cudaMemcpy(w->h_ctl, d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost));
+    w->h_ctl->wsel = s.wsel;
+    w->h_ctl->wcount[s.wsel] = s.wcount;
+    NE_CUDA_TRY(cudaMemcpy(d.ctl, w->h_ctl, sizeof(neb::Ctl), cudaMemcpyHostToDevice));
+    w->stats = s.stats;
+    return NE_OK;
+}
+
+}  // extern "C"
+
+struct NeCheckpoint {
+    const NeWorld* owner = nullptr;
+    uint32_t n = 0;
+    Saved s;
+};
+
+extern "C" {
+
+int ne_world_checkpoint(NeWorld* w, NeCheckpoint** out) {
+    if (!w || !out) return set_err(NE_ERR_ARG, "NULL argument");
+    *out = nullptr;
+    if (!w->has_bodies) return set_err(NE_ERR_ARG, "world has no bodies");
+    NE_CUDA_TRY(cudaSetDevice(w->device));
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    NeCheckpoint* ck = new NeCheckpoint;
+    ck->owner = w;
+    ck->n = w->n;
+    int rc = save_state(w, ck->s);
+    if (rc != NE_OK) {
+        saved_free(ck->s);
+        delete ck;
+        return rc;
+    }
+    *out = ck;
+    return NE_OK;
+}
+
+int ne_world_restore(NeWorld* w, const NeCheckpoint* ck) {
+    if (!w || !ck) return set_err(NE_ERR_ARG, "NULL argument");
+    if (ck->owner != w) return set_err(NE_ERR_ARG, "checkpoint belongs to another world");
+    if (ck->n != w->n) return set_err(NE_ERR_ARG, "body count changed since the checkpoint");
+    NE_CUDA_TRY(cudaSetDevice(w->device));
+    return restore_state(w, ck->s);
+}
+
+int ne_checkpoint_destroy(NeCheckpoint* ck) {
+    if (!ck) return NE_OK;
+    saved_free(ck->s);
+    delete ck;
+    return NE_OK;
+}
+
+int ne_world_autotune(NeWorld* w, uint32_t steps, NeSolverShape* chosen) {
+    if (!w) return set_err(NE_ERR_ARG, "world is NULL");
+    if (!w->has_bodies) return set_err(NE_ERR_ARG, "world has no bodies");
+    NE_CUDA_TRY(cudaSetDevice(w->device));
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    if (steps == 0) steps = 1;
+    static const NeSolverShape cand[] = {{512, 1}, {256, 1}, {256, 2}, {128, 1}, {128, 2}, {128, 4}};
+    const bool prof = w->profile;
+    w->profile = false;
+    Saved s;
+    int rc = save_state(w, s);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    NeSolverShape best = {w->big_threads, w->big_ctas_per_sm};
+    float best_ms = -1.0f;
+    if (rc == NE_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        rc = set_err(NE_ERR_CUDA, "cudaEventCreate failed");
+    // One untimed pass first, so buffer growth does not land in a timing.
+    if (rc == NE_OK && (rc = ne_world_step(w, steps)) == NE_OK) rc = restore_state(w, s);
+    for (const NeSolverShape& c : cand) {
+        if (rc != NE_OK) break;
+        w->big_threads = c.threads;
+        w->big_ctas_per_sm = c.ctas_per_sm;
+        cudaEventRecord(e0, w->stream);
+        if ((rc = ne_world_step(w, steps)) != NE_OK) break;
+        cudaEventRecord(e1, w->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (best_ms < 0.0f || ms < best_ms) { best_ms = ms; best = c; }
+        rc = restore_state(w, s);
+    }
+    if (rc != NE_OK) restore_state(w, s);
+    w->big_threads = best.threads;
+    w->big_ctas_per_sm = best.ctas_per_sm;
+    w->profile = prof;
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    saved_free(s);
+    if (rc == NE_OK && chosen) *chosen = best;
+    return rc;
 }
 
 int ne_world_set_record(NeWorld* w, uint32_t flags) {

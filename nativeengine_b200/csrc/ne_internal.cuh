@@ -96,6 +96,17 @@ struct DevWorld {
     uint32_t* bstart;        // [n] first rank entry of each body in the sorted entries
     uint32_t* bcnt10;        // [10C] unfinished-predecessor counts of the solver updates
     uint32_t* bq10;          // [10C] ready queues of the solver updates
+    // batched FP32 form (null in FP64 mode): FP32 copies of the body state the
+    // narrowphase and the solver read, refreshed every step after integration,
+    // and the FP32 constraint records.  Poses, the warm-start impulses and the
+    // body state between steps stay in the FP64 arrays above.
+    F4 *f_v, *f_w;           // [n] (v, invMass), (omega, -): solver working state
+    F4 *f_q;                 // [n] orientation (w, x, y, z)
+    F4 *f_I;                 // [n] (invI, halfHeight)
+    F4 *f_e;                 // [n] (half extents or plane normal, radius)
+    F4* f_verts;             // convex vertices (body frame)
+    F4 *f_n, *f_ra, *f_rb;   // [C] (n, overlap), (rA, restBias), (rB, mu)
+    float* f_kn;             // [C] effective mass along n
     // scratch
     uint32_t *hist, *tsum;
     Ctl* ctl;

@@ -14,9 +14,7 @@
 // Every kernel is a no-op once ctl->abort is set (a capacity overflow this
 // step); the host then restores the pre-step snapshot, grows the buffer and
 // re-runs the step, so an overflow never changes the result.
-#include <cuda/atomic>
-
-#include "ne_step.cuh"
+#include "ne_solve.cuh"
 
 namespace neb {
 
@@ -282,6 +280,15 @@ __global__ void __launch_bounds__(kT) k_integrate(StepArgs a) {
     d.omg[i] = d4of(wv, 0.0);
     d.frc[i] = d4of(F, 0.0);
     d.trq[i] = d4of(T, 0.0);
+    if (a.f32) {
+        // FP32 working copies for the narrowphase and the solver.
+        const D4 I = d.inert[i], g = d.geom[i], e = d.ext[i];
+        d.f_v[i] = F4{(float)v.x, (float)v.y, (float)v.z, (float)invM};
+        d.f_w[i] = F4{(float)wv.x, (float)wv.y, (float)wv.z, 0.0f};
+        d.f_q[i] = F4{(float)q.w, (float)q.x, (float)q.y, (float)q.z};
+        d.f_I[i] = F4{(float)I.x, (float)I.y, (float)I.z, (float)g.y};
+        d.f_e[i] = F4{(float)e.x, (float)e.y, (float)e.z, (float)g.x};
+    }
 }
 
 __global__ void __launch_bounds__(kT) k_ext_reset(StepArgs a) {
@@ -700,11 +707,20 @@ __global__ void __launch_bounds__(kT) k_constraint_build(StepArgs a) {
         d.cj[c] = j;
         d.cslot[c] = k;
         d.con_n[c] = cn;
-        d.con_ra[c] = d4of(rA, restBias);
-        d.con_rb[c] = d4of(rB, mu);
         d.con_p[c] = d4of(pt, 0.0);
         d.con_imp[c] = make_double2(nImp, 0.0);
-        d.con_kn[c] = eff_mass_at(d, i, j, rA, rB, n);
+        const double Kn = eff_mass_at(d, i, j, rA, rB, n);
+        if (a.f32) {
+            // FP32 solver records (built from FP64 operands, then rounded).
+            d.f_n[c] = F4{(float)n.x, (float)n.y, (float)n.z, (float)cn.w};
+            d.f_ra[c] = F4{(float)rA.x, (float)rA.y, (float)rA.z, (float)restBias};
+            d.f_rb[c] = F4{(float)rB.x, (float)rB.y, (float)rB.z, (float)mu};
+            d.f_kn[c] = (float)Kn;
+        } else {
+            d.con_ra[c] = d4of(rA, restBias);
+            d.con_rb[c] = d4of(rB, mu);
+            d.con_kn[c] = Kn;
+        }
         d.wkey[ws ^ 1][c] = key;
     }
 }
@@ -737,10 +753,7 @@ __global__ void __launch_bounds__(kT) k_island_mark(StepArgs a, int ib) {
     a.d.iflag[k] = f;
 }
 
-// Island segments; islands with at least kBigIsland contacts are queued for
-// the dataflow solver, the rest are solved one thread per island.
-constexpr uint32_t kBigIsland = 48;
-
+// Island segments.
 __global__ void __launch_bounds__(kT) k_island_start(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
@@ -909,191 +922,20 @@ __device__ __forceinline__ void correct_item(const DevWorld& d, uint32_t c, doub
     if (wimp_out) wimp_out[c] = d.con_imp[c].x;
 }
 
-// One thread per small island: warm start (src/world.cpp:559-568), 8
-// Gauss-Seidel sweeps in the reference's contact order (:572-612), position
-// correction (:615-616), warm-cache values (:619-626).  Islands share no
-// mutable body, so concurrent islands reproduce the reference's single
-// global sweep exactly.  Big islands are queued for k_island_solve_big.
-__global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
-    Ctl* ctl = a.d.ctl;
-    if (ctl->abort) return;
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= ctl->islands) return;
-    const DevWorld& d = a.d;
-    const uint32_t s = d.istart[t], e = d.istart[t + 1];
-    atomicMax((unsigned long long*)&ctl->max_island, (unsigned long long)(e - s));
-    if (e - s >= kBigIsland) {
-        const uint32_t slot = atomicAdd(&ctl->nbig, 1u);
-        d.big[slot] = (uint32_t)t;
-        return;
+struct ItemsF64 {
+    static __device__ __forceinline__ void warm(const DevWorld& d, uint32_t c) { warm_item(d, c); }
+    static __device__ __forceinline__ void sweep(const DevWorld& d, uint32_t c) { sweep_item(d, c); }
+    static __device__ __forceinline__ void correct(const DevWorld& d, uint32_t c, double beta, double* wout) {
+        correct_item(d, c, beta, wout);
     }
-    const uint32_t* ord = d.iord[ib];
-    if (a.warm)
-        for (uint32_t k = s; k < e; ++k) warm_item(d, ord[k]);
-    for (int it = 0; it < 8; ++it)
-        for (uint32_t k = s; k < e; ++k) sweep_item(d, ord[k]);
-    double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
-    const double beta = a.wp[a.bw[d.ci[ord[s]]]].beta;
-    for (uint32_t k = s; k < e; ++k) correct_item(d, ord[k], beta, wout);
-}
-
-// A warp that sees no update complete for this long gives up and reports
-// (ctl->solve_timeout -> NE_ERR_TIMEOUT).  Legitimate waits are bounded by the
-// island's critical path, well under a millisecond per update.
-constexpr unsigned long long kStallNs = 2000000000ull;
-constexpr uint32_t kEmpty = 0xffffffffu;
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-constexpr int kBigThreads = 512;
-
-// Island-local view of one contact's update (phase p, contact position pos).
-struct BigItem {
-    uint32_t c, i, j, pos, p;
-    bool mi, mj;
 };
 
-__device__ __forceinline__ BigItem big_item(const DevWorld& d, const uint32_t* ord, uint32_t s, uint32_t m,
-                                            uint32_t u) {
-    BigItem it;
-    it.p = u / m;
-    it.pos = s + (u - it.p * m);
-    it.c = ord[it.pos];
-    it.i = d.ci[it.c];
-    it.j = d.cj[it.c];
-    it.mi = (d.meta[it.i].y & kFlagMutable) != 0;
-    it.mj = (d.meta[it.j].y & kFlagMutable) != 0;
-    return it;
+__global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
+    solve::island_solve_small<ItemsF64>(a, ib);
 }
 
-// Number of earlier updates this update waits for: one per mutable body,
-// except a body's very first update (phase 0, rank 0).
-__device__ __forceinline__ uint32_t big_npred(const DevWorld& d, const BigItem& it) {
-    uint32_t n = 0;
-    if (it.mi && !(it.p == 0 && d.crank[2 * it.pos] == 0)) ++n;
-    if (it.mj && !(it.p == 0 && d.crank[2 * it.pos + 1] == 0)) ++n;
-    return n;
-}
-
-// The update that follows this one on body b (side 0 = i, 1 = j), or kEmpty.
-__device__ __forceinline__ uint32_t big_successor(const DevWorld& d, const uint32_t* rv, const BigItem& it, int side,
-                                                  uint32_t b, uint32_t s, uint32_t m) {
-    const uint32_t r = d.crank[2 * it.pos + side];
-    const uint32_t deg = d.bdeg[b];
-    const uint32_t base = d.bstart[b];
-    if (r + 1 < deg) return it.p * m + ((rv[base + r + 1] >> 1) - s);
-    if (it.p < 9) return (it.p + 1) * m + ((rv[base] >> 1) - s);
-    return kEmpty;
-}
-
-__device__ __forceinline__ void big_push(uint32_t* queue, uint32_t* tail, uint32_t u) {
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> t(*tail);
-    const uint32_t slot = t.fetch_add(1u, cuda::memory_order_relaxed);
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> q(queue[slot]);
-    q.store(u, cuda::memory_order_release);
-}
-
-__device__ __forceinline__ void big_notify(uint32_t* cnt, uint32_t* queue, uint32_t* tail, uint32_t u) {
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> c(cnt[u]);
-    if (c.fetch_sub(1u, cuda::memory_order_acq_rel) == 1u) big_push(queue, tail, u);
-}
-
-// Dataflow solver for the big islands, one CTA per island.
-//
-// The reference's work on an island is a sequence of 10*m updates (phase 0 =
-// warm start, phases 1-8 = the Gauss-Seidel sweeps, phase 9 = position
-// correction; m contacts in order).  An update reads and writes only its two
-// bodies, so it depends only on the previous update of each of those bodies
-// in that sequence.  Each update counts its unfinished predecessors (<= 2);
-// finishing an update decrements its successors' counts, and the update that
-// reaches zero is appended to a ready queue.  Lanes claim queue slots in order
-// and run the update in a slot once it is filled.  Every body therefore sees
-// exactly the reference's sequence of updates (bit-identical result), and the
-// schedule is greedy list scheduling, whose length is close to the
-// dependency graph's critical path.  Progress is guaranteed: while updates
-// remain, some update is ready, and the lowest unfilled slot is claimed by a
-// waiting lane.  Lanes poll warp-synchronously (no lane spins alone, so a
-// ready update is never starved by divergent waiters), and every wait is
-// bounded and reports through ctl->solve_timeout.
-__global__ void __launch_bounds__(kBigThreads) k_island_solve_big(StepArgs a, int ib, int rb) {
-    Ctl* ctl = a.d.ctl;
-    if (ctl->abort) return;
-    __shared__ int s_fail;
-    __shared__ uint32_t s_head, s_tail;
-    const DevWorld& d = a.d;
-    const uint32_t* ord = d.iord[ib];
-    const uint32_t* rv = d.rval[rb];
-    double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
-    const uint32_t nbig = ctl->nbig;
-    for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
-        const uint32_t t = d.big[bi];
-        const uint32_t s = d.istart[t], e = d.istart[t + 1];
-        const uint32_t m = e - s;
-        const uint32_t total = 10u * m;
-        const double beta = a.wp[a.bw[d.ci[ord[s]]]].beta;
-        uint32_t* cnt = d.bcnt10 + 10u * s;      // per-island slices of the 10*C scratch
-        uint32_t* queue = d.bq10 + 10u * s;
-        if (threadIdx.x == 0) { s_fail = 0; s_head = 0; s_tail = 0; }
-        for (uint32_t u = threadIdx.x; u < total; u += blockDim.x) {
-            cnt[u] = big_npred(d, big_item(d, ord, s, m, u));
-            queue[u] = kEmpty;
-        }
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x)
-            if (cnt[k] == 0) big_push(queue, &s_tail, k);
-        __syncthreads();
-
-        cuda::atomic_ref<uint32_t, cuda::thread_scope_block> head(s_head);
-        uint32_t h = head.fetch_add(1u, cuda::memory_order_relaxed);
-        unsigned long long last_progress = global_ns();
-        uint32_t rounds = 0;
-        while (true) {
-            const bool live = h < total;
-            if (!__any_sync(0xffffffffu, live)) break;
-            uint32_t u = kEmpty;
-            if (live) {
-                cuda::atomic_ref<uint32_t, cuda::thread_scope_block> q(queue[h]);
-                u = q.load(cuda::memory_order_acquire);
-            }
-            const bool ready = u != kEmpty;
-            if (ready) {
-                const BigItem it = big_item(d, ord, s, m, u);
-                if (it.p == 0) {
-                    if (a.warm) warm_item(d, it.c);
-                } else if (it.p <= 8) {
-                    sweep_item(d, it.c);
-                } else {
-                    correct_item(d, it.c, beta, wout);
-                }
-                const uint32_t si = it.mi ? big_successor(d, rv, it, 0, it.i, s, m) : kEmpty;
-                const uint32_t sj = it.mj ? big_successor(d, rv, it, 1, it.j, s, m) : kEmpty;
-                if (si != kEmpty) big_notify(cnt, queue, &s_tail, si);
-                if (sj != kEmpty) big_notify(cnt, queue, &s_tail, sj);
-                h = head.fetch_add(1u, cuda::memory_order_relaxed);
-            }
-            // Check the clock every 64 idle rounds; lane 0's reading decides
-            // for the warp so the exit is warp-uniform.
-            bool stalled = false;
-            if (__any_sync(0xffffffffu, ready)) {
-                rounds = 0;
-                last_progress = global_ns();
-            } else if ((++rounds & 63u) == 0u) {
-                stalled = __shfl_sync(0xffffffffu, global_ns() - last_progress > kStallNs ? 1 : 0, 0) != 0;
-            }
-            const bool failed = __any_sync(0xffffffffu, *(volatile int*)&s_fail != 0);   // warp-uniform
-            if (stalled || failed) {
-                if ((threadIdx.x & 31) == 0) {
-                    s_fail = 1;
-                    atomicExch(&ctl->solve_timeout, 1u);
-                }
-                break;
-            }
-        }
-        __syncthreads();
-    }
+__global__ void __launch_bounds__(solve::kMaxBigThreads) k_island_solve_big(StepArgs a, int ib, int rb) {
+    solve::island_solve_big<ItemsF64>(a, ib, rb);
 }
 
 // wrapPositions() / applyWalls() (src/world.cpp:698-702, 635-657).
@@ -1192,7 +1034,11 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
     scan_u32(d.pflag, d.poff, (uint32_t)a.Pcap, d.tsum, &ctl->S, ctl, st, launches);
     k_compact<<<blocks_for(a.Pcap, kT), kT, 0, st>>>(a); ++L;
     mark(3);
-    k_narrowphase<<<blocks_for(a.Scap, 128), 128, 0, st>>>(a); ++L;
+    if (a.f32) {
+        launch_narrowphase_f32(a, st, launches);
+    } else {
+        k_narrowphase<<<blocks_for(a.Scap, 128), 128, 0, st>>>(a); ++L;
+    }
     mark(4);
     scan_u32(d.ccnt, d.coff, (uint32_t)a.Scap, d.tsum, &ctl->C, ctl, st, launches);
     k_constraint_build<<<blocks_for(a.Scap, kT), kT, 0, st>>>(a); ++L;
@@ -1215,8 +1061,12 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
     const int rb = radix_sort_u32(rks, rvs, (uint32_t)(2 * a.Ccap), lbits, d.hist, d.tsum, ctl, st, launches);
     k_rank_write<<<blocks_for(2 * a.Ccap, kT), kT, 0, st>>>(a, rb); ++L;
     mark(6);
-    k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib); ++L;
-    k_island_solve_big<<<a.num_sms, kBigThreads, 0, st>>>(a, ib, rb); ++L;
+    if (a.f32) {
+        launch_solve_f32(a, ib, rb, st, launches);
+    } else {
+        k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib); ++L;
+        k_island_solve_big<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb); ++L;
+    }
     mark(7);
     k_boundary<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
     k_step_end<<<1, 1, 0, st>>>(a); ++L;

@@ -21,9 +21,11 @@ def _ptr(a: Optional[np.ndarray]):
 
 class DeviceWorld:
     def __init__(self, params: Optional[_ffi.NeWorldParams] = None, bodies: Optional[BodyArrays] = None,
-                 record: bool = True):
+                 record: bool = True, precision: str = "f64"):
         """record=True keeps the reference-rule pair list of every step for
-        pairs() (the parity tests need it); benchmarks pass record=False."""
+        pairs() (the parity tests need it); benchmarks pass record=False.
+        precision: "f64" (bit-exact with the reference) or "f32" (the batched
+        FP32 form)."""
         self._lib = _ffi.load()
         self.params = params if params is not None else default_params()
         h = C.c_void_p()
@@ -32,6 +34,7 @@ class DeviceWorld:
         self.n = 0
         if record:
             _ffi.check(self._lib.ne_world_set_record(self._h, _ffi.RECORD_PAIRS), "ne_world_set_record")
+        self.set_precision(precision)
         if bodies is not None:
             self.upload(bodies)
 
@@ -140,6 +143,36 @@ class DeviceWorld:
         _ffi.check(self._lib.ne_world_islands(self._h, _ptr(lab), self.n), "ne_world_islands")
         return lab
 
+    def set_precision(self, precision: str):
+        code = {"f64": _ffi.PRECISION_F64, "f32": _ffi.PRECISION_F32}[precision]
+        _ffi.check(self._lib.ne_world_set_precision(self._h, code), "ne_world_set_precision")
+        self.precision = precision
+
+    def solver_shape(self):
+        s = _ffi.NeSolverShape()
+        _ffi.check(self._lib.ne_world_get_solver_shape(self._h, C.byref(s)), "ne_world_get_solver_shape")
+        return int(s.threads), int(s.ctas_per_sm)
+
+    def set_solver_shape(self, threads: int, ctas_per_sm: int = 1):
+        s = _ffi.NeSolverShape(threads, ctas_per_sm)
+        _ffi.check(self._lib.ne_world_set_solver_shape(self._h, C.byref(s)), "ne_world_set_solver_shape")
+
+    def autotune(self, steps: int = 5):
+        """Time the big-island solver's launch shapes from the current state,
+        keep the fastest; the state is left as it was."""
+        s = _ffi.NeSolverShape()
+        _ffi.check(self._lib.ne_world_autotune(self._h, steps, C.byref(s)), "ne_world_autotune")
+        return int(s.threads), int(s.ctas_per_sm)
+
+    def checkpoint(self) -> "Checkpoint":
+        """Device copy of the state and the warm cache (see restore())."""
+        h = C.c_void_p()
+        _ffi.check(self._lib.ne_world_checkpoint(self._h, C.byref(h)), "ne_world_checkpoint")
+        return Checkpoint(self._lib, h)
+
+    def restore(self, ck: "Checkpoint"):
+        _ffi.check(self._lib.ne_world_restore(self._h, ck._h), "ne_world_restore")
+
     def profile(self, enable: bool = True):
         _ffi.check(self._lib.ne_world_profile(self._h, 1 if enable else 0), "ne_world_profile")
 
@@ -160,3 +193,22 @@ class DeviceWorld:
         v = C.c_uint64()
         _ffi.check(self._lib.ne_world_launch_count(self._h, C.byref(v)), "ne_world_launch_count")
         return int(v.value)
+
+
+class Checkpoint:
+    """Owned handle of an NeCheckpoint; destroy it before its world."""
+
+    def __init__(self, lib, h):
+        self._lib = lib
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ne_checkpoint_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
