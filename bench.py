@@ -387,7 +387,7 @@ def run_ours(args):
             "dtype": "f64" if args.precision == "f64" else "f32 (FP64 poses, wrap, warm impulses, EPA tests)",
             "data": "synthetic",
             "config": {"workload": workload, "bodies": n, "steps_per_run": K, "precision": args.precision,
-                       "solver_shape": {"threads": shape[0], "ctas_per_sm": shape[1],
+                       "solver_shape": {"threads": shape[0], "ctas_per_sm": shape[1], "team_max": shape[2],
                                         "autotuned": bool(args.autotune)},
                        "parallelism": "replicas" if world > 1 else "single world",
                        "l2": "256 MiB buffer rewritten between timed steps (outside the events)"},

@@ -244,9 +244,13 @@ int ne_world_islands(NeWorld* world, uint32_t* label, uint32_t n);
 #define NE_PRECISION_F32 1
 int ne_world_set_precision(NeWorld* world, int precision);
 
-/* Launch shape of the big-island solver (islands of >= 48 contacts, one CTA
- * per island at a time).  No counterpart in the reference.  Results do not
- * depend on it.  threads: 128, 256 or 512; ctas_per_sm: 1..4.
+/* Launch shape of the big-island solver (islands of >= 48 contacts).  No
+ * counterpart in the reference.  Results do not depend on it.
+ * threads: 128, 256 or 512 per CTA; ctas_per_sm: 1..4;
+ * team_max: 1 = each big island is solved by one CTA (ready queue in shared
+ * memory); 2..64 = an island may be solved by a team of up to team_max CTAs
+ * on different SMs (queue and counters in global memory), sized in proportion
+ * to its share of the work.
  * ne_world_autotune times each candidate shape for `steps` steps from the
  * current state, keeps the fastest and restores the state and warm cache, so
  * the world continues as if it had not been called; *chosen (may be NULL)
@@ -254,6 +258,7 @@ int ne_world_set_precision(NeWorld* world, int precision);
 typedef struct NeSolverShape {
     uint32_t threads;
     uint32_t ctas_per_sm;
+    uint32_t team_max;
 } NeSolverShape;
 int ne_world_set_solver_shape(NeWorld* world, const NeSolverShape* shape);
 int ne_world_get_solver_shape(const NeWorld* world, NeSolverShape* shape);

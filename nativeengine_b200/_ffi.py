@@ -89,7 +89,7 @@ class NeContactArrays(C.Structure):
 
 
 class NeSolverShape(C.Structure):
-    _fields_ = [("threads", C.c_uint32), ("ctas_per_sm", C.c_uint32)]
+    _fields_ = [("threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("team_max", C.c_uint32)]
 
 
 class NeStepStats(C.Structure):

@@ -82,12 +82,13 @@ struct NeWorld {
     int precision = NE_PRECISION_F64;
     uint32_t big_threads = 512;           // big-island solver launch shape
     uint32_t big_ctas_per_sm = 1;
+    uint32_t big_team_max = 1;
     size_t nverts = 0;                    // convex vertex pool entries on the device
     uint64_t Rcap = 0;                    // capacity of the recorded pair list
     int key_bits = 64;
     int num_sms = 148;
     // capacities (entries)
-    uint64_t Pcap = 0, Scap = 0, Ccap = 0;
+    uint64_t Scap = 0, Ccap = 0;
     size_t nverts_alloc = 0, nnc_alloc = 0, nplanes_alloc = 0;
     std::vector<double> h_invmass;   // for upload_state packing
     std::vector<neb::D4> stage;      // host packing buffer (uploads)
@@ -112,6 +113,8 @@ void free_body_arrays(NeWorld* w) {
     dfree(d.s_pos); dfree(d.s_quat); dfree(d.s_vel); dfree(d.s_omg); dfree(d.s_frc); dfree(d.s_trq);
     dfree(d.key[0]); dfree(d.key[1]); dfree(d.val[0]); dfree(d.val[1]);
     dfree(d.bcnt); dfree(d.boff); dfree(d.parent); dfree(d.bdeg); dfree(d.bstart);
+    dfree(d.cflag); dfree(d.crun); dfree(d.cstart); dfree(d.hkey); dfree(d.hval); dfree(d.bstage); dfree(d.srec);
+    d.hsize = 0;
     dfree(d.f_v); dfree(d.f_w); dfree(d.f_q); dfree(d.f_I); dfree(d.f_e); dfree(d.f_verts);
 }
 
@@ -145,11 +148,6 @@ int alloc_f32_cons(NeWorld* w, uint64_t cap) {
     return NE_OK;
 }
 
-void free_pair_arrays(NeWorld* w) {
-    neb::DevWorld& d = w->d;
-    dfree(d.pair_i); dfree(d.pair_j); dfree(d.pflag); dfree(d.poff);
-}
-
 int alloc_rec(NeWorld* w, uint64_t cap) {
     neb::DevWorld& d = w->d;
     dfree(d.rec_i);
@@ -162,7 +160,7 @@ int alloc_rec(NeWorld* w, uint64_t cap) {
 
 void free_surv_arrays(NeWorld* w) {
     neb::DevWorld& d = w->d;
-    dfree(d.surv); dfree(d.ccnt); dfree(d.coff); dfree(d.cn); dfree(d.cp);
+    dfree(d.si); dfree(d.sj); dfree(d.stage_j); dfree(d.ccnt); dfree(d.coff); dfree(d.cn); dfree(d.cp);
 }
 
 void free_con_arrays(NeWorld* w) {
@@ -171,7 +169,7 @@ void free_con_arrays(NeWorld* w) {
     dfree(d.con_imp); dfree(d.ilab[0]); dfree(d.ilab[1]); dfree(d.iord[0]); dfree(d.iord[1]); dfree(d.iflag);
     dfree(d.ioff); dfree(d.istart); dfree(d.big); dfree(d.con_kn);
     dfree(d.rkey[0]); dfree(d.rkey[1]); dfree(d.rval[0]); dfree(d.rval[1]); dfree(d.crank);
-    dfree(d.bcnt10); dfree(d.bq10);
+    dfree(d.bcnt10); dfree(d.bq10); dfree(d.bctl); dfree(d.bteam);
     free_f32_cons(w);
 }
 
@@ -181,21 +179,10 @@ int alloc_scratch(NeWorld* w) {
     dfree(d.tsum);
     uint64_t sortn = std::max<uint64_t>(w->n, 2 * w->Ccap);
     size_t hw = neb::radix_hist_words((uint32_t)sortn);
-    uint64_t scann = std::max<uint64_t>(std::max<uint64_t>(w->Pcap, w->Scap), std::max<uint64_t>(hw, sortn));
+    uint64_t scann = std::max<uint64_t>(w->Scap, std::max<uint64_t>(hw, sortn));
     int rc;
     if ((rc = dalloc(&d.hist, hw)) != NE_OK) return rc;
     if ((rc = dalloc(&d.tsum, neb::scan_tsum_words((uint32_t)scann) + 8)) != NE_OK) return rc;
-    return NE_OK;
-}
-
-int alloc_pairs(NeWorld* w, uint64_t cap) {
-    free_pair_arrays(w);
-    neb::DevWorld& d = w->d;
-    int rc;
-    if ((rc = dalloc(&d.pair_i, cap)) || (rc = dalloc(&d.pair_j, cap)) || (rc = dalloc(&d.pflag, cap)) ||
-        (rc = dalloc(&d.poff, cap)))
-        return rc;
-    w->Pcap = cap;
     return NE_OK;
 }
 
@@ -203,7 +190,9 @@ int alloc_surv(NeWorld* w, uint64_t cap) {
     free_surv_arrays(w);
     neb::DevWorld& d = w->d;
     int rc;
-    if ((rc = dalloc(&d.surv, cap)) || (rc = dalloc(&d.ccnt, cap)) || (rc = dalloc(&d.coff, cap)) ||
+    if ((rc = dalloc(&d.si, cap)) || (rc = dalloc(&d.sj, cap)) || (rc = dalloc(&d.stage_j, cap)) ||
+        (rc = dalloc(&d.ccnt, cap)) ||
+        (rc = dalloc(&d.coff, cap)) ||
         (rc = dalloc(&d.cn, 4 * cap)) || (rc = dalloc(&d.cp, 4 * cap)))
         return rc;
     w->Scap = cap;
@@ -224,7 +213,8 @@ int alloc_cons(NeWorld* w, uint64_t cap) {
         (rc = dalloc(&d.big, cap)) || (rc = dalloc(&d.con_kn, cap)) || (rc = dalloc(&d.rkey[0], 2 * cap)) ||
         (rc = dalloc(&d.rkey[1], 2 * cap)) || (rc = dalloc(&d.rval[0], 2 * cap)) ||
         (rc = dalloc(&d.rval[1], 2 * cap)) || (rc = dalloc(&d.crank, 2 * cap)) ||
-        (rc = dalloc(&d.bcnt10, 10 * cap)) || (rc = dalloc(&d.bq10, 10 * cap)))
+        (rc = dalloc(&d.bcnt10, 10 * cap)) || (rc = dalloc(&d.bq10, 10 * cap)) ||
+        (rc = dalloc(&d.bctl, cap / neb::kBigIsland + 1)) || (rc = dalloc(&d.bteam, cap / neb::kBigIsland + 2)))
         return rc;
     if (w->precision == NE_PRECISION_F32 && (rc = alloc_f32_cons(w, cap))) return rc;
     unsigned long long* nk[2] = {nullptr, nullptr};
@@ -268,7 +258,7 @@ neb::StepArgs make_args(const NeWorld* w) {
     a.f32 = w->precision == NE_PRECISION_F32 ? 1 : 0;
     a.big_threads = (int)w->big_threads;
     a.big_ctas_per_sm = (int)w->big_ctas_per_sm;
-    a.Pcap = w->Pcap;
+    a.big_team_max = (int)w->big_team_max;
     a.Scap = w->Scap;
     a.Ccap = w->Ccap;
     a.Rcap = w->Rcap;
@@ -469,7 +459,6 @@ int ne_world_destroy(NeWorld* w) {
     if (!w) return NE_OK;
     if (w->stream) cudaStreamSynchronize(w->stream);
     free_body_arrays(w);
-    free_pair_arrays(w);
     free_surv_arrays(w);
     free_con_arrays(w);
     neb::DevWorld& d = w->d;
@@ -558,8 +547,14 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
             (rc = dalloc(&d.s_trq, m)) || (rc = dalloc(&d.key[0], m)) || (rc = dalloc(&d.key[1], m)) ||
             (rc = dalloc(&d.val[0], m)) || (rc = dalloc(&d.val[1], m)) || (rc = dalloc(&d.bcnt, m)) ||
             (rc = dalloc(&d.boff, m)) || (rc = dalloc(&d.parent, m)) || (rc = dalloc(&d.bdeg, m)) ||
-            (rc = dalloc(&d.bstart, m)))
+            (rc = dalloc(&d.bstart, m)) || (rc = dalloc(&d.cflag, m)) || (rc = dalloc(&d.crun, m)) ||
+            (rc = dalloc(&d.cstart, m + 1)) || (rc = dalloc(&d.bstage, m)) || (rc = dalloc(&d.srec, m)))
             return rc;
+        // Cell hash table: a power of two >= 2n slots (load factor <= 1/2).
+        uint32_t hs = 64;
+        while (hs < 2 * m) hs <<= 1;
+        if ((rc = dalloc(&d.hkey, hs)) || (rc = dalloc(&d.hval, hs))) return rc;
+        d.hsize = hs;
     }
     // Pack the host arrays into the 32-byte device records.
     std::vector<neb::D4>& st = w->stage;
@@ -674,10 +669,9 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
     if ((rc = derive_worlds(w, planes))) return rc;
 
     // Initial capacities; they grow on demand (see ne_world_step).
-    if (!w->Pcap) {
-        // Typical contact-rich scenes: ~60 grid candidates, ~4 surviving pairs
-        // and ~5 contacts per body; larger needs grow (a re-run step).
-        if ((rc = alloc_pairs(w, std::max<uint64_t>(64ull * n, 4096)))) return rc;
+    if (!w->Scap) {
+        // Typical contact-rich scenes: ~4 surviving pairs and ~5 contacts per
+        // body; larger needs grow (a re-run step).
         if ((rc = alloc_surv(w, std::max<uint64_t>(6ull * n, 1024)))) return rc;
         if ((rc = alloc_cons(w, std::max<uint64_t>(8ull * n, 1024)))) return rc;
     }
@@ -816,11 +810,8 @@ int ne_world_step(NeWorld* w, uint32_t nsteps) {
                 if (c.P_ref > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 recorded pairs");
                 if ((rc = alloc_rec(w, grow_to(c.P_ref)))) return rc;
                 grew = true;
-            } else if (c.P > w->Pcap) {
-                if (c.P > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 candidate pairs");
-                if ((rc = alloc_pairs(w, grow_to(c.P)))) return rc;
-                grew = true;
             } else if (c.S > w->Scap) {
+                if (c.S > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 surviving pairs");
                 if ((rc = alloc_surv(w, grow_to(c.S)))) return rc;
                 grew = true;
             } else if (c.C > w->Ccap) {
@@ -961,8 +952,10 @@ int ne_world_set_solver_shape(NeWorld* w, const NeSolverShape* s) {
     if (s->threads != 128 && s->threads != 256 && s->threads != 512)
         return set_err(NE_ERR_ARG, "solver threads must be 128, 256 or 512");
     if (s->ctas_per_sm < 1 || s->ctas_per_sm > 4) return set_err(NE_ERR_ARG, "solver ctas_per_sm must be 1..4");
+    if (s->team_max < 1 || s->team_max > 64) return set_err(NE_ERR_ARG, "solver team_max must be 1..64");
     w->big_threads = s->threads;
     w->big_ctas_per_sm = s->ctas_per_sm;
+    w->big_team_max = s->team_max;
     return NE_OK;
 }
 
@@ -970,6 +963,7 @@ int ne_world_get_solver_shape(const NeWorld* w, NeSolverShape* s) {
     if (!w || !s) return set_err(NE_ERR_ARG, "NULL argument");
     s->threads = w->big_threads;
     s->ctas_per_sm = w->big_ctas_per_sm;
+    s->team_max = w->big_team_max;
     return NE_OK;
 }
 
@@ -1082,13 +1076,14 @@ int ne_world_autotune(NeWorld* w, uint32_t steps, NeSolverShape* chosen) {
     NE_CUDA_TRY(cudaSetDevice(w->device));
     NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
     if (steps == 0) steps = 1;
-    static const NeSolverShape cand[] = {{512, 1}, {256, 1}, {256, 2}, {128, 1}, {128, 2}, {128, 4}};
+    static const NeSolverShape cand[] = {{512, 1, 1}, {256, 1, 1}, {256, 2, 1}, {128, 1, 1}, {128, 2, 1},
+                                         {128, 4, 1}, {256, 1, 4}, {256, 1, 16}, {128, 2, 8}};
     const bool prof = w->profile;
     w->profile = false;
     Saved s;
     int rc = save_state(w, s);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    NeSolverShape best = {w->big_threads, w->big_ctas_per_sm};
+    NeSolverShape best = {w->big_threads, w->big_ctas_per_sm, w->big_team_max};
     float best_ms = -1.0f;
     if (rc == NE_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
         rc = set_err(NE_ERR_CUDA, "cudaEventCreate failed");
@@ -1098,6 +1093,7 @@ int ne_world_autotune(NeWorld* w, uint32_t steps, NeSolverShape* chosen) {
         if (rc != NE_OK) break;
         w->big_threads = c.threads;
         w->big_ctas_per_sm = c.ctas_per_sm;
+        w->big_team_max = c.team_max;
         cudaEventRecord(e0, w->stream);
         if ((rc = ne_world_step(w, steps)) != NE_OK) break;
         cudaEventRecord(e1, w->stream);
@@ -1110,6 +1106,7 @@ int ne_world_autotune(NeWorld* w, uint32_t steps, NeSolverShape* chosen) {
     if (rc != NE_OK) restore_state(w, s);
     w->big_threads = best.threads;
     w->big_ctas_per_sm = best.ctas_per_sm;
+    w->big_team_max = best.team_max;
     w->profile = prof;
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);

@@ -13,7 +13,8 @@
 //                ext  = (halfExtents | plane normal, -)
 //                mat  = (friction, restitution, linearDamping, angularDamping)
 //                meta = (shape, flags, layer, mask)
-//   pairs    : CSR by first body -- pair_i/pair_j in sorted (i, j) order.
+//   pairs    : surviving pairs si/sj, CSR by first body, in sorted (i, j) order
+//              (rec_i/rec_j: the reference-rule list, when recording).
 //   contacts : 4 slots per surviving pair (normal+depth, point).
 //   constraints, warm cache, island order: flat arrays in solver order.
 #pragma once
@@ -41,13 +42,27 @@ struct Ctl {
     uint32_t need_bits;      // sort-key bits the cell keys needed
     uint32_t local_bits;     // widest per-world cell-key layout this step
     uint32_t wsel;           // warm cache buffer holding the previous step
-    uint64_t P, S, C;        // candidate pairs, survivors, contacts (totals, even if over capacity)
+    uint64_t P, S, C;        // grid candidates examined, surviving pairs, contacts (totals, even if over capacity)
     uint64_t P_ref;          // pairs of the reference's broadphase rule (recorded steps)
     uint64_t islands, max_island, epa_cap_hits;
     uint32_t nbig;           // islands solved by the dataflow kernel this step
     uint32_t solve_timeout;  // a bounded dependency wait ran out (error)
     uint32_t wcount[2];      // warm cache entries per buffer
     uint64_t scan_total;     // scratch total of the last scan
+    uint64_t sort_hist_len;  // live length of the radix sort's digit histogram
+    uint64_t C2;             // 2 * C: rank entries of the dataflow solver
+    uint64_t ncells;         // runs of equal cell keys after the sort (internal grid)
+    uint64_t S_stage;        // surviving pairs staged so far this step
+};
+
+// Islands with at least kBigIsland contacts go to the team (dataflow)
+// solver; smaller ones are solved one thread per island.
+constexpr uint32_t kBigIsland = 48;
+
+// Big-island solver control block: ready-queue head (claims) and tail
+// (pushes), updates done, failure flag.
+struct BigCtl {
+    uint32_t head, tail, done, fail;
 };
 
 struct DevWorld {
@@ -67,10 +82,18 @@ struct DevWorld {
     unsigned long long *key[2];
     uint32_t* val[2];
     uint32_t *bcnt, *boff;
-    uint32_t *pair_i, *pair_j;     // internal candidate pairs (CSR by first body)
+    // cell table of the internal grid: run r of equal sorted keys occupies
+    // sorted positions [cstart[r], cstart[r+1]); an open-addressing hash maps
+    // a cell key to its run
+    uint32_t *cflag, *crun, *cstart;   // [n], [n], [n + 1]
+    unsigned long long* hkey;          // [hsize] (~0 = empty)
+    uint32_t* hval;                    // [hsize]
+    uint32_t hsize;                    // power of two >= 2n
+    uint32_t *stage_j, *bstage;        // [Scap] staged partner lists, [n] staging offset per body
+    D4* srec;                          // [n] (x, y, z, boundR) in sorted cell order
     uint32_t *rec_i, *rec_j;       // reference-rule pair list (recorded steps only)
-    // narrowphase
-    uint32_t *pflag, *poff, *surv;
+    // narrowphase: the pairs that pass the filters and the cull, sorted by (i, j)
+    uint32_t *si, *sj;
     uint32_t *ccnt, *coff;
     D4 *cn, *cp;             // 4 slots per survivor: (normal, depth), (point, -)
     // constraints
@@ -96,6 +119,8 @@ struct DevWorld {
     uint32_t* bstart;        // [n] first rank entry of each body in the sorted entries
     uint32_t* bcnt10;        // [10C] unfinished-predecessor counts of the solver updates
     uint32_t* bq10;          // [10C] ready queues of the solver updates
+    BigCtl* bctl;            // [C/48 + 1] per big island
+    uint32_t* bteam;         // [C/48 + 2] first virtual CTA of each big island's team
     // batched FP32 form (null in FP64 mode): FP32 copies of the body state the
     // narrowphase and the solver read, refreshed every step after integration,
     // and the FP32 constraint records.  Poses, the warm-start impulses and the
@@ -112,22 +137,21 @@ struct DevWorld {
     Ctl* ctl;
 };
 
-struct Caps {
-    uint64_t P, S, C;
-};
-
 // Scan / sort primitives (ne_prims.cu).  All are asynchronous on `st`, all skip
 // when ctl->abort is set, and all count their launches into *launches.
 // Exclusive scan of n u32 values; the u64 total lands in *total (device).
+// n is the capacity; with n_dev only the first min(n, *n_dev) elements count.
 void scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tsum, uint64_t* total,
-              const Ctl* ctl, cudaStream_t st, uint64_t* launches);
+              const Ctl* ctl, cudaStream_t st, uint64_t* launches, const uint64_t* n_dev = nullptr);
 size_t scan_tsum_words(uint32_t n);
 // Stable LSD radix sort of (key, val) pairs on the low `bits` bits.
 // Ping-pongs between buffers 0 and 1; returns the buffer index holding the result.
 int radix_sort_u64(unsigned long long* key[2], uint32_t* val[2], uint32_t n, int bits, uint32_t* hist,
-                   uint32_t* tsum, const Ctl* ctl, cudaStream_t st, uint64_t* launches);
+                   uint32_t* tsum, const Ctl* ctl, cudaStream_t st, uint64_t* launches,
+                   const uint64_t* n_dev = nullptr);
 int radix_sort_u32(uint32_t* key[2], uint32_t* val[2], uint32_t n, int bits, uint32_t* hist,
-                   uint32_t* tsum, const Ctl* ctl, cudaStream_t st, uint64_t* launches);
+                   uint32_t* tsum, const Ctl* ctl, cudaStream_t st, uint64_t* launches,
+                   const uint64_t* n_dev = nullptr);
 size_t radix_hist_words(uint32_t n);
 
 }  // namespace neb

@@ -5,6 +5,10 @@
 // warp sub-tile with __match_any_sync in element order, so equal keys keep
 // their input order (stability is what keeps bodies in a cell, and contacts in
 // an island, in the reference's index order).
+//
+// Both take a host-side capacity n (launch size) and an optional device-side
+// count n_dev: only the first min(n, *n_dev) elements are scanned or sorted,
+// so a buffer sized for the worst case costs only what the step filled.
 #include "ne_internal.cuh"
 
 namespace neb {
@@ -46,12 +50,24 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t& excl, 
     return total;
 }
 
+__device__ __forceinline__ uint32_t live_count(uint32_t n, const uint64_t* n_dev) {
+    if (!n_dev) return n;
+    const uint64_t v = *n_dev;
+    return v < (uint64_t)n ? (uint32_t)v : n;
+}
+
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t* __restrict__ in,
-                                                             uint32_t* __restrict__ out, uint32_t n,
+                                                             uint32_t* __restrict__ out, uint32_t ncap,
                                                              uint32_t* __restrict__ tsum,
-                                                             const Ctl* __restrict__ ctl) {
+                                                             const Ctl* __restrict__ ctl,
+                                                             const uint64_t* __restrict__ n_dev) {
     if (ctl->abort) return;
     __shared__ uint32_t sm[33];
+    const uint32_t n = live_count(ncap, n_dev);
+    if ((uint64_t)blockIdx.x * kScanTile >= n) {
+        if (threadIdx.x == 0) tsum[blockIdx.x] = 0u;
+        return;
+    }
     const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
     uint32_t x[kScanItems];
     uint32_t s = 0;
@@ -92,9 +108,10 @@ __global__ void __launch_bounds__(kTopThreads) k_scan_top(uint32_t* __restrict__
     if (threadIdx.x == 0) *total = carry;
 }
 
-__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_t* __restrict__ tsum,
-                           const Ctl* __restrict__ ctl) {
+__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t ncap, const uint32_t* __restrict__ tsum,
+                           const Ctl* __restrict__ ctl, const uint64_t* __restrict__ n_dev) {
     if (ctl->abort) return;
+    const uint32_t n = live_count(ncap, n_dev);
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] += tsum[i / kScanTile];
 }
@@ -109,14 +126,22 @@ __device__ __forceinline__ int digit_of(K k, int shift) {
     return (int)((k >> shift) & (K)0xFF);
 }
 
+// Digit histogram per 256-element sub-tile, laid out [digit][sub-tile] over
+// the live sub-tiles; block 0 publishes that layout's length for the scan.
 template <typename K>
-__global__ void __launch_bounds__(kSortWarps * 32) k_radix_hist(const K* __restrict__ keys, uint32_t n,
+__global__ void __launch_bounds__(kSortWarps * 32) k_radix_hist(const K* __restrict__ keys, uint32_t ncap,
                                                                 int shift, uint32_t* __restrict__ hist,
-                                                                uint32_t nsub, const Ctl* __restrict__ ctl) {
+                                                                const Ctl* __restrict__ ctl,
+                                                                const uint64_t* __restrict__ n_dev,
+                                                                uint64_t* __restrict__ hist_len) {
     if (ctl->abort) return;
     __shared__ uint32_t cnt[kSortWarps][256];
+    const uint32_t n = live_count(ncap, n_dev);
+    const uint32_t nsub = (n + kSub - 1) / kSub;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *hist_len = 256ull * nsub;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t g = blockIdx.x * kSortWarps + w;
+    if (blockIdx.x * kSortWarps >= nsub) return;
     for (int d = lane; d < 256; d += 32) cnt[w][d] = 0u;
     __syncwarp();
     if (g < nsub) {
@@ -135,11 +160,14 @@ template <typename K>
 __global__ void __launch_bounds__(kSortWarps * 32) k_radix_scatter(const K* __restrict__ kin,
                                                                    const uint32_t* __restrict__ vin,
                                                                    K* __restrict__ kout, uint32_t* __restrict__ vout,
-                                                                   uint32_t n, int shift,
-                                                                   const uint32_t* __restrict__ hist, uint32_t nsub,
-                                                                   const Ctl* __restrict__ ctl) {
+                                                                   uint32_t ncap, int shift,
+                                                                   const uint32_t* __restrict__ hist,
+                                                                   const Ctl* __restrict__ ctl,
+                                                                   const uint64_t* __restrict__ n_dev) {
     if (ctl->abort) return;
     __shared__ uint32_t cnt[kSortWarps][256];
+    const uint32_t n = live_count(ncap, n_dev);
+    const uint32_t nsub = (n + kSub - 1) / kSub;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t g = blockIdx.x * kSortWarps + w;
     if (g >= nsub) return;
@@ -168,19 +196,20 @@ inline uint32_t ceil_div(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1)
 
 template <typename K>
 int radix_sort_impl(K* key[2], uint32_t* val[2], uint32_t n, int bits, uint32_t* hist, uint32_t* tsum,
-                    const Ctl* ctl, cudaStream_t st, uint64_t* launches) {
+                    const Ctl* ctl, cudaStream_t st, uint64_t* launches, const uint64_t* n_dev) {
     int cur = 0;
     if (n <= 1 || bits <= 0) return cur;
     const uint32_t nsub = ceil_div(n, kSub);
     const uint32_t nblk = ceil_div(nsub, kSortWarps);
     const uint32_t hn = 256u * nsub;
     uint64_t* total = const_cast<uint64_t*>(&ctl->scan_total);
+    uint64_t* hlen = const_cast<uint64_t*>(&ctl->sort_hist_len);
     for (int shift = 0; shift < bits; shift += 8) {
-        k_radix_hist<K><<<nblk, kSortWarps * 32, 0, st>>>(key[cur], n, shift, hist, nsub, ctl);
+        k_radix_hist<K><<<nblk, kSortWarps * 32, 0, st>>>(key[cur], n, shift, hist, ctl, n_dev, hlen);
         ++*launches;
-        scan_u32(hist, hist, hn, tsum, total, ctl, st, launches);
+        scan_u32(hist, hist, hn, tsum, total, ctl, st, launches, hlen);
         k_radix_scatter<K><<<nblk, kSortWarps * 32, 0, st>>>(key[cur], val[cur], key[cur ^ 1], val[cur ^ 1], n,
-                                                              shift, hist, nsub, ctl);
+                                                              shift, hist, ctl, n_dev);
         ++*launches;
         cur ^= 1;
     }
@@ -193,26 +222,26 @@ size_t scan_tsum_words(uint32_t n) { return (size_t)ceil_div(n, kScanTile) + 1; 
 size_t radix_hist_words(uint32_t n) { return (size_t)256 * ceil_div(n, kSub) + 1; }
 
 void scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tsum, uint64_t* total, const Ctl* ctl,
-              cudaStream_t st, uint64_t* launches) {
+              cudaStream_t st, uint64_t* launches, const uint64_t* n_dev) {
     if (n == 0) return;
     const uint32_t ntiles = ceil_div(n, kScanTile);
-    k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(in, out, n, tsum, ctl);
+    k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(in, out, n, tsum, ctl, n_dev);
     k_scan_top<<<1, kTopThreads, 0, st>>>(tsum, ntiles, total, ctl);
     *launches += 2;
     if (ntiles > 1) {
-        k_scan_add<<<ceil_div(n, 256), 256, 0, st>>>(out, n, tsum, ctl);
+        k_scan_add<<<ceil_div(n, 256), 256, 0, st>>>(out, n, tsum, ctl, n_dev);
         ++*launches;
     }
 }
 
 int radix_sort_u64(unsigned long long* key[2], uint32_t* val[2], uint32_t n, int bits, uint32_t* hist,
-                   uint32_t* tsum, const Ctl* ctl, cudaStream_t st, uint64_t* launches) {
-    return radix_sort_impl<unsigned long long>(key, val, n, bits, hist, tsum, ctl, st, launches);
+                   uint32_t* tsum, const Ctl* ctl, cudaStream_t st, uint64_t* launches, const uint64_t* n_dev) {
+    return radix_sort_impl<unsigned long long>(key, val, n, bits, hist, tsum, ctl, st, launches, n_dev);
 }
 
 int radix_sort_u32(uint32_t* key[2], uint32_t* val[2], uint32_t n, int bits, uint32_t* hist, uint32_t* tsum,
-                   const Ctl* ctl, cudaStream_t st, uint64_t* launches) {
-    return radix_sort_impl<uint32_t>(key, val, n, bits, hist, tsum, ctl, st, launches);
+                   const Ctl* ctl, cudaStream_t st, uint64_t* launches, const uint64_t* n_dev) {
+    return radix_sort_impl<uint32_t>(key, val, n, bits, hist, tsum, ctl, st, launches, n_dev);
 }
 
 }  // namespace neb

@@ -11,9 +11,10 @@
 //   Items::sweep(d, c)                  one sequential-impulse update of c
 //   Items::correct(d, c, beta, wout)    position correction of c + warm-cache value
 //
-// Small islands run one thread each, in order.  Big islands run on the
-// dataflow scheduler below, which gives every body exactly the sequence of
-// updates the in-order loop would, so both drivers compute the same bits.
+// Small islands run one thread each, in order.  Big islands run on one of the
+// dataflow schedulers below (one CTA per island, or a team of CTAs), which give
+// every body exactly the sequence of updates the in-order loop would, so all
+// drivers compute the same bits.
 #pragma once
 
 #include <cuda/atomic>
@@ -22,10 +23,6 @@
 
 namespace neb {
 namespace solve {
-
-// Islands with at least kBigIsland contacts are queued for the dataflow
-// solver, the rest are solved one thread per island.
-constexpr uint32_t kBigIsland = 48;
 
 // A warp that sees no update complete for this long gives up and reports
 // (ctl->solve_timeout -> NE_ERR_TIMEOUT).  Legitimate waits are bounded by the
@@ -79,23 +76,11 @@ __device__ __forceinline__ uint32_t big_successor(const DevWorld& d, const uint3
     return kEmpty;
 }
 
-__device__ __forceinline__ void big_push(uint32_t* queue, uint32_t* tail, uint32_t u) {
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> t(*tail);
-    const uint32_t slot = t.fetch_add(1u, cuda::memory_order_relaxed);
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> q(queue[slot]);
-    q.store(u, cuda::memory_order_release);
-}
-
-__device__ __forceinline__ void big_notify(uint32_t* cnt, uint32_t* queue, uint32_t* tail, uint32_t u) {
-    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> c(cnt[u]);
-    if (c.fetch_sub(1u, cuda::memory_order_acq_rel) == 1u) big_push(queue, tail, u);
-}
-
 // One thread per small island: warm start (src/world.cpp:559-568), 8
 // Gauss-Seidel sweeps in the reference's contact order (:572-612), position
 // correction (:615-616), warm-cache values (:619-626).  Islands share no
 // mutable body, so concurrent islands reproduce the reference's single
-// global sweep exactly.  Big islands are queued for island_solve_big.
+// global sweep exactly.  Big islands are queued for the dataflow solvers.
 template <class Items>
 __device__ __forceinline__ void island_solve_small(const StepArgs& a, int ib) {
     Ctl* ctl = a.d.ctl;
@@ -120,7 +105,20 @@ __device__ __forceinline__ void island_solve_small(const StepArgs& a, int ib) {
     for (uint32_t k = s; k < e; ++k) Items::correct(d, ord[k], beta, wout);
 }
 
-// Dataflow solver for the big islands, one CTA per island at a time.
+__device__ __forceinline__ void big_push(uint32_t* queue, uint32_t* tail, uint32_t u) {
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> t(*tail);
+    const uint32_t slot = t.fetch_add(1u, cuda::memory_order_relaxed);
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> q(queue[slot]);
+    q.store(u, cuda::memory_order_release);
+}
+
+__device__ __forceinline__ void big_notify(uint32_t* cnt, uint32_t* queue, uint32_t* tail, uint32_t u) {
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_block> c(cnt[u]);
+    if (c.fetch_sub(1u, cuda::memory_order_acq_rel) == 1u) big_push(queue, tail, u);
+}
+
+// Block-local dataflow solver: one CTA per big island at a time, ready queue
+// head/tail in shared memory and block-scope atomics (team size 1).
 //
 // The reference's work on an island is a sequence of 10*m updates (phase 0 =
 // warm start, phases 1-8 = the Gauss-Seidel sweeps, phase 9 = position
@@ -138,7 +136,7 @@ __device__ __forceinline__ void island_solve_small(const StepArgs& a, int ib) {
 // ready update is never starved by divergent waiters), and every wait is
 // bounded and reports through ctl->solve_timeout.
 template <class Items>
-__device__ __forceinline__ void island_solve_big(const StepArgs& a, int ib, int rb) {
+__device__ __forceinline__ void island_solve_local(const StepArgs& a, int ib, int rb) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     __shared__ int s_fail;
@@ -213,6 +211,274 @@ __device__ __forceinline__ void island_solve_big(const StepArgs& a, int ib, int 
             }
         }
         __syncthreads();
+    }
+}
+
+// ---- big islands: a team of CTAs per island --------------------------------
+//
+// The reference's work on an island is a sequence of 10*m updates (phase 0 =
+// warm start, phases 1-8 = the Gauss-Seidel sweeps, phase 9 = position
+// correction; m contacts in order).  An update reads and writes only its two
+// bodies, so it depends only on the previous update of each of those bodies
+// in that sequence.  Each update counts its unfinished predecessors (<= 2);
+// finishing an update decrements its successors' counts.  Every body
+// therefore sees exactly the reference's sequence of updates (bit-identical
+// result) whatever the schedule.
+//
+// Schedule: the lane whose decrement makes a successor ready runs it next
+// itself (a continuation), so chains along the critical path never pass
+// through a queue; a second ready successor is appended to the island's ready
+// queue.  Idle lanes claim queue slots in order (one atomic per warp) and run
+// the update in a slot once it is filled.  All counters, the queue and the
+// mutable body state live in global memory with device-scope acquire/release
+// ordering and L2-coherent loads, so an island can be worked on by a team of
+// CTAs on many SMs: k_big_plan gives each big island a team proportional to
+// its update count (at least one CTA; islands beyond the grid are taken in
+// turn).  Progress: the lowest unfinished update is ready, and it is either a
+// lane's continuation or in a queue slot that is, or will next be, claimed by
+// a waiting lane.  Lanes poll warp-synchronously, and every wait is bounded
+// and reports through ctl->solve_timeout.
+
+// Coherent (L2) access to solver state that another SM may have written.
+__device__ __forceinline__ D4 ldcg(const D4* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = __ldcg(q), b = __ldcg(q + 1);
+    D4 r; r.x = a.x; r.y = a.y; r.z = b.x; r.w = b.y;
+    return r;
+}
+__device__ __forceinline__ void stcg(D4* p, const D4& v) {
+    double2* q = reinterpret_cast<double2*>(p);
+    __stcg(q, make_double2(v.x, v.y));
+    __stcg(q + 1, make_double2(v.z, v.w));
+}
+__device__ __forceinline__ F4 ldcg(const F4* p) {
+    const float4 a = __ldcg(reinterpret_cast<const float4*>(p));
+    F4 r; r.x = a.x; r.y = a.y; r.z = a.z; r.w = a.w;
+    return r;
+}
+__device__ __forceinline__ void stcg(F4* p, const F4& v) {
+    __stcg(reinterpret_cast<float4*>(p), make_float4(v.x, v.y, v.z, v.w));
+}
+__device__ __forceinline__ double2 ldcg(const double2* p) { return __ldcg(p); }
+__device__ __forceinline__ void stcg(double2* p, const double2& v) { __stcg(p, v); }
+
+// Loads and stores of mutable solver state: plain for the one-thread small
+// islands, coherent for the team solver.
+template <bool Coherent, typename T>
+__device__ __forceinline__ T ld_state(const T* p) {
+    if constexpr (Coherent) return ldcg(p); else return *p;
+}
+template <bool Coherent, typename T>
+__device__ __forceinline__ void st_state(T* p, const T& v) {
+    if constexpr (Coherent) stcg(p, v); else *p = v;
+}
+
+// Island k of the team that virtual CTA v belongs to (bteam: team starts).
+__device__ __forceinline__ uint32_t team_island(const uint32_t* bteam, uint32_t nbig, uint32_t v) {
+    uint32_t lo = 0, hi = nbig - 1;   // last k with bteam[k] <= v
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        if (bteam[mid] <= v) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Teams (single block of kPlanThreads): island k gets
+// clamp(floor(G * m_k / sum m), 1, team_max) of the G CTAs; bteam = exclusive
+// prefix of team sizes, bteam[nbig] = number of virtual CTAs.
+constexpr int kPlanThreads = 1024;
+
+__device__ __forceinline__ void big_plan(const StepArgs& a, uint32_t G) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const DevWorld& d = a.d;
+    const uint32_t nbig = ctl->nbig;
+    __shared__ unsigned long long s_sum[kPlanThreads / 32];
+    __shared__ unsigned long long s_total;
+    __shared__ uint32_t s_warp[kPlanThreads / 32], s_carry;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned long long acc = 0;
+    for (uint32_t k = threadIdx.x; k < nbig; k += blockDim.x) {
+        const uint32_t t = d.big[k];
+        acc += d.istart[t + 1] - d.istart[t];
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) s_sum[w] = acc;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long tot = 0;
+        for (int k = 0; k < kPlanThreads / 32; ++k) tot += s_sum[k];
+        s_total = tot ? tot : 1;
+    }
+    __syncthreads();
+    const unsigned long long W = s_total;
+    for (uint32_t base = 0; base < nbig; base += blockDim.x) {
+        const uint32_t k = base + threadIdx.x;
+        uint32_t team = 0;
+        if (k < nbig) {
+            const uint32_t t = d.big[k];
+            const unsigned long long mk = d.istart[t + 1] - d.istart[t];
+            team = (uint32_t)((unsigned long long)G * mk / W);
+            team = team < 1u ? 1u : team;
+            if (a.big_team_max > 0 && team > (uint32_t)a.big_team_max) team = (uint32_t)a.big_team_max;
+        }
+        uint32_t inc = team;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += x;
+        }
+        if (lane == 31) s_warp[w] = inc;
+        __syncthreads();
+        if (w == 0) {
+            const uint32_t x = s_warp[lane];
+            uint32_t xi = x;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, xi, o);
+                if (lane >= o) xi += y;
+            }
+            s_warp[lane] = xi - x;
+        }
+        __syncthreads();
+        if (k < nbig) d.bteam[k] = s_carry + s_warp[w] + inc - team;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) s_carry += s_warp[w] + inc;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) d.bteam[nbig] = s_carry;
+}
+
+// Predecessor counts, an empty queue with the initially ready updates, and
+// the control block of every big island; one block per island at a time.
+__device__ __forceinline__ void big_init(const StepArgs& a, int ib) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const DevWorld& d = a.d;
+    const uint32_t nbig = ctl->nbig;
+    const uint32_t* ord = d.iord[ib];
+    __shared__ uint32_t s_tail;
+    for (uint32_t k = blockIdx.x; k < nbig; k += gridDim.x) {
+        const uint32_t t = d.big[k];
+        const uint32_t s = d.istart[t], e = d.istart[t + 1];
+        const uint32_t m = e - s;
+        const uint32_t total = 10u * m;
+        uint32_t* cnt = d.bcnt10 + 10u * s;
+        uint32_t* queue = d.bq10 + 10u * s;
+        if (threadIdx.x == 0) s_tail = 0;
+        for (uint32_t u = threadIdx.x; u < total; u += blockDim.x) {
+            cnt[u] = big_npred(d, big_item(d, ord, s, m, u));
+            queue[u] = kEmpty;
+        }
+        __syncthreads();
+        for (uint32_t u = threadIdx.x; u < m; u += blockDim.x)   // only phase 0 can start ready
+            if (cnt[u] == 0) queue[atomicAdd(&s_tail, 1u)] = u;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            BigCtl c;
+            c.head = 0; c.tail = s_tail; c.done = 0; c.fail = 0;
+            d.bctl[k] = c;
+        }
+        __syncthreads();
+    }
+}
+
+template <class Items>
+__device__ __forceinline__ void island_solve_team(const StepArgs& a, int ib, int rb) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const DevWorld& d = a.d;
+    const uint32_t nbig = ctl->nbig;
+    if (nbig == 0) return;
+    const uint32_t* ord = d.iord[ib];
+    const uint32_t* rv = d.rval[rb];
+    double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t nvirt = d.bteam[nbig];
+    constexpr uint32_t kNone = 0xfffffffeu;
+    for (uint32_t v = blockIdx.x; v < nvirt; v += gridDim.x) {
+        const uint32_t k = team_island(d.bteam, nbig, v);
+        const uint32_t t = d.big[k];
+        const uint32_t s = d.istart[t], e = d.istart[t + 1];
+        const uint32_t m = e - s;
+        const uint32_t total = 10u * m;
+        const double beta = a.wp[a.bw[d.ci[ord[s]]]].beta;
+        uint32_t* cnt = d.bcnt10 + 10u * s;
+        uint32_t* queue = d.bq10 + 10u * s;
+        BigCtl* bc = d.bctl + k;
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> head(bc->head), tail(bc->tail), done(bc->done),
+            fail(bc->fail);
+        uint32_t cont = kEmpty, slot = kNone;
+        unsigned long long last_progress = global_ns();
+        uint32_t rounds = 0;
+        while (true) {
+            // Lanes without work claim the next queue slots (one atomic per warp).
+            const bool need = cont == kEmpty && slot == kNone;
+            const uint32_t nb = __ballot_sync(0xffffffffu, need);
+            if (nb) {
+                uint32_t base = 0;
+                if (lane == __ffs(nb) - 1) base = head.fetch_add((uint32_t)__popc(nb), cuda::memory_order_relaxed);
+                base = __shfl_sync(0xffffffffu, base, __ffs(nb) - 1);
+                if (need) slot = base + __popc(nb & lt);
+            }
+            uint32_t u = cont;
+            cont = kEmpty;
+            if (u == kEmpty && slot < total) {
+                cuda::atomic_ref<uint32_t, cuda::thread_scope_device> q(queue[slot]);
+                const uint32_t x = q.load(cuda::memory_order_acquire);
+                if (x != kEmpty) { u = x; slot = kNone; }
+            }
+            const bool ready = u != kEmpty;
+            if (ready) {
+                const BigItem it = big_item(d, ord, s, m, u);
+                if (it.p == 0) {
+                    if (a.warm) Items::warm(d, it.c);
+                } else if (it.p <= 8) {
+                    Items::sweep(d, it.c);
+                } else {
+                    Items::correct(d, it.c, beta, wout);
+                }
+                const uint32_t si = it.mi ? big_successor(d, rv, it, 0, it.i, s, m) : kEmpty;
+                const uint32_t sj = it.mj ? big_successor(d, rv, it, 1, it.j, s, m) : kEmpty;
+                #pragma unroll
+                for (int side = 0; side < 2; ++side) {
+                    const uint32_t nx = side ? sj : si;
+                    if (nx == kEmpty) continue;
+                    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> c(cnt[nx]);
+                    if (c.fetch_sub(1u, cuda::memory_order_acq_rel) != 1u) continue;
+                    if (cont == kEmpty) {
+                        cont = nx;
+                    } else {
+                        const uint32_t sl = tail.fetch_add(1u, cuda::memory_order_relaxed);
+                        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> q(queue[sl]);
+                        q.store(nx, cuda::memory_order_release);
+                    }
+                }
+            }
+            const uint32_t rb_ = __ballot_sync(0xffffffffu, ready);
+            if (rb_ && lane == __ffs(rb_) - 1) done.fetch_add((uint32_t)__popc(rb_), cuda::memory_order_release);
+            if (rb_) {
+                rounds = 0;
+                last_progress = global_ns();
+                continue;
+            }
+            if (__any_sync(0xffffffffu, cont != kEmpty)) continue;
+            // Idle warp: finished island, failure elsewhere, or a stall.
+            ++rounds;   // warp-uniform
+            int stop = 0;
+            if (lane == 0) {
+                if (done.load(cuda::memory_order_acquire) >= total) stop = 1;
+                else if (fail.load(cuda::memory_order_relaxed)) stop = 1;
+                else if ((rounds & 63u) == 0u && global_ns() - last_progress > kStallNs) stop = 2;
+            }
+            stop = __shfl_sync(0xffffffffu, stop, 0);
+            if (stop == 2 && lane == 0) {
+                fail.store(1u, cuda::memory_order_relaxed);
+                atomicExch(&ctl->solve_timeout, 1u);
+            }
+            if (stop) break;
+            if (rounds >= 16) __nanosleep(64);   // long idle: ease the polling traffic
+        }
     }
 }
 

@@ -2,8 +2,9 @@
 //
 // Stage map (reference -> kernel):
 //   integrate()            src/world.cpp:373-411   k_integrate
-//   broadphasePairs()      src/world.cpp:424-501   k_cell_keys, radix sort, k_pair_count, k_pair_emit
-//   pair filters + cull    src/world.cpp:513-516   k_pair_cull, k_compact
+//   broadphasePairs()      src/world.cpp:424-501   k_cell_keys, radix sort, cell table (k_cell_flags,
+//                                                  k_cell_table); reference-rule list: k_pair_count, k_pair_emit
+//   pair filters + cull    src/world.cpp:513-516   k_surv_gather, k_surv_place (fused with the pair lists)
 //   gatherContacts()       src/world.cpp:88-130    k_narrowphase (ne_geom.cuh)
 //   constraint build       src/world.cpp:537-553   k_constraint_build (+ union-find hooking)
 //   islands                src/world.cpp:332-343   k_island_label, radix sort, k_island_mark/_start
@@ -226,6 +227,7 @@ __global__ void k_step_begin(Ctl* ctl) {
     ctl->epa_cap_hits = 0;
     ctl->nbig = 0;
     ctl->solve_timeout = 0;
+    ctl->S_stage = 0;
 }
 
 __device__ __forceinline__ long long warp_min_ll(long long v) {
@@ -414,42 +416,24 @@ __global__ void __launch_bounds__(kT) k_pair_count(StepArgs a, int kb, int fast)
     d.bcnt[i] = cnt;
 }
 
-// Writes body i's sorted partner list at its CSR offset.  One warp per body.
-// The partner candidates are up to 27 sorted runs (one per distinct
-// neighbour cell; members with index > i) plus the sorted run of the world's
-// excluded bodies > i.  Lanes split the concatenated candidates evenly; each
-// candidate's output rank is its index in its own run plus the number of
-// smaller candidates in the other runs (all candidates are distinct bodies).
-__global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb, int fast, uint32_t* out_i, uint32_t* out_j,
-                                                  const uint64_t* total_p, uint64_t cap) {
-    Ctl* ctl = a.d.ctl;
-    if (ctl->abort) return;
-    if (*total_p > cap) {
-        if (threadIdx.x == 0 && blockIdx.x == 0) ctl->abort = 1;
-        return;
-    }
-    __shared__ uint32_t s_lo[kT / 32][28], s_len[kT / 32][28], s_ex[kT / 32][29];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= a.n) return;
-    const DevWorld& d = a.d;
-    const uint32_t w = a.bw[i];
-    const WorldP& W = a.wp[w];
-    const GridSel G = grid_sel(a, W, fast);
-    const uint32_t base = d.boff[i];
-    if (G.brute || excluded(d.meta[i], fast)) {
-        const uint32_t cnt = W.end - 1 - i;
-        for (uint32_t k = lane; k < cnt; k += 32) {
-            out_i[base + k] = i;
-            out_j[base + k] = i + 1 + k;
-        }
-        return;
-    }
-    const KeyLayout L = key_layout(a, w, G, (int)ctl->local_bits);
-    const D4 p = d.pos[i];
+// Candidate partners j > i of grid body i, as up to 28 sorted runs: one per
+// distinct neighbour cell (its members with index > i) and, last, the world's
+// excluded bodies > i.  Every lane of the warp calls this; the runs land in
+// the warp's shared slots lo/len/ex (ex = exclusive offset of each run in the
+// concatenated candidate sequence, ex[nr] = total).
+struct Runs {
+    uint32_t total;
+    int nr;
+    bool xl_last;      // the last run is the excluded list
+};
+
+__device__ __forceinline__ Runs warp_runs(const StepArgs& a, const WorldP& W, const GridSel& G, const KeyLayout& L,
+                                          uint32_t i, const D4& p, int kb, uint32_t* lo_s, uint32_t* len_s,
+                                          uint32_t* ex_s) {
+    const int lane = threadIdx.x & 31;
     const long long cx = cell_of(W, G, p.x, 0), cy = cell_of(W, G, p.y, 1), cz = cell_of(W, G, p.z, 2);
-    const unsigned long long* keys = d.key[kb];
-    const uint32_t* vals = d.val[kb];
+    const unsigned long long* keys = a.d.key[kb];
+    const uint32_t* vals = a.d.val[kb];
     // Lane t < 27 takes neighbour offset t (duplicates from wrap aliasing keep
     // their lowest lane); lane 27 takes the excluded list.
     uint32_t rlo = 0, rhi = 0;
@@ -477,33 +461,77 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb, int fast, 
         uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    const int nr = __popc(nonempty);
-    // The excluded run (lane 27) is the last non-empty run if present.
-    const bool xl_nonempty = (nonempty >> 27) & 1u;
+    Runs R;
+    R.total = __shfl_sync(0xffffffffu, incl, 31);
+    R.nr = __popc(nonempty);
+    R.xl_last = (nonempty >> 27) & 1u;
     if (len > 0) {
-        s_lo[wid][r] = rlo;
-        s_len[wid][r] = len;
-        s_ex[wid][r] = incl - len;
+        lo_s[r] = rlo;
+        len_s[r] = len;
+        ex_s[r] = incl - len;
     }
-    if (lane == 0) s_ex[wid][nr] = total;
+    if (lane == 0) ex_s[R.nr] = R.total;
     __syncwarp();
-    for (uint32_t e = lane; e < total; e += 32) {
-        // Owning run: last r with s_ex[r] <= e.
-        int lo = 0, hi = nr - 1;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (s_ex[wid][mid] <= e) lo = mid; else hi = mid - 1;
+    return R;
+}
+
+// Candidate number e of the concatenated runs: its body index, owning run and
+// index within that run.
+__device__ __forceinline__ uint32_t run_candidate(const Runs& R, const uint32_t* lo_s, const uint32_t* ex_s,
+                                                  const uint32_t* vals, const uint32_t* xl, uint32_t e, int& own,
+                                                  uint32_t& idx) {
+    int lo = 0, hi = R.nr - 1;   // owning run: last r with ex[r] <= e
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (ex_s[mid] <= e) lo = mid; else hi = mid - 1;
+    }
+    own = lo;
+    idx = e - ex_s[own];
+    const bool own_xl = R.xl_last && own == R.nr - 1;
+    return own_xl ? xl[lo_s[own] + idx] : vals[lo_s[own] + idx];
+}
+
+// Writes body i's sorted partner list at its CSR offset (the reference-rule
+// list of recorded steps).  One warp per body.  Each candidate's output rank is
+// its index in its own run plus the number of smaller candidates in the other
+// runs (all candidates are distinct bodies).
+__global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb, int fast, uint32_t* out_i, uint32_t* out_j,
+                                                  const uint64_t* total_p, uint64_t cap) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    if (*total_p > cap) {
+        if (threadIdx.x == 0 && blockIdx.x == 0) ctl->abort = 1;
+        return;
+    }
+    __shared__ uint32_t s_lo[kT / 32][28], s_len[kT / 32][28], s_ex[kT / 32][29];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= a.n) return;
+    const DevWorld& d = a.d;
+    const uint32_t w = a.bw[i];
+    const WorldP& W = a.wp[w];
+    const GridSel G = grid_sel(a, W, fast);
+    const uint32_t base = d.boff[i];
+    if (G.brute || excluded(d.meta[i], fast)) {
+        const uint32_t cnt = W.end - 1 - i;
+        for (uint32_t k = lane; k < cnt; k += 32) {
+            out_i[base + k] = i;
+            out_j[base + k] = i + 1 + k;
         }
-        const int own = lo;
-        const uint32_t idx = e - s_ex[wid][own];
-        const bool own_xl = xl_nonempty && own == nr - 1;
-        const uint32_t x = own_xl ? G.xl[s_lo[wid][own] + idx] : vals[s_lo[wid][own] + idx];
+        return;
+    }
+    const KeyLayout L = key_layout(a, w, G, (int)ctl->local_bits);
+    const uint32_t* vals = d.val[kb];
+    const Runs R = warp_runs(a, W, G, L, i, d.pos[i], kb, s_lo[wid], s_len[wid], s_ex[wid]);
+    for (uint32_t e = lane; e < R.total; e += 32) {
+        int own;
+        uint32_t idx;
+        const uint32_t x = run_candidate(R, s_lo[wid], s_ex[wid], vals, G.xl, e, own, idx);
         uint32_t rank = idx;
-        for (int q = 0; q < nr; ++q) {
+        for (int q = 0; q < R.nr; ++q) {
             if (q == own) continue;
             const uint32_t ql = s_lo[wid][q], qh = ql + s_len[wid][q];
-            const uint32_t* src = (xl_nonempty && q == nr - 1) ? G.xl : vals;
+            const uint32_t* src = (R.xl_last && q == R.nr - 1) ? G.xl : vals;
             rank += lower_bound_u32(src, ql, qh, x) - ql;
         }
         out_i[base + rank] = i;
@@ -511,66 +539,352 @@ __global__ void __launch_bounds__(kT) k_pair_emit(StepArgs a, int kb, int fast, 
     }
 }
 
-
 // Pair filters (src/world.cpp:513-516) and a conservative bounding-volume cull
 // that only removes pairs the narrowphase provably reports as separated.
-__global__ void __launch_bounds__(kT) k_pair_cull(StepArgs a) {
+// CullA holds the first body's operands, loaded once per partner list.
+struct CullA {
+    V3 x;
+    double invM, r;
+    uint4 m;
+    uint2 nr;
+    Q q;
+    V3 he;
+    Domain dom;
+};
+
+__device__ __forceinline__ CullA cull_self(const StepArgs& a, uint32_t i) {
+    const DevWorld& d = a.d;
+    CullA A;
+    const D4 p = d.pos[i];
+    A.x = v3of(p);
+    A.invM = p.w;
+    A.r = d.inert[i].w;
+    A.m = d.meta[i];
+    A.nr = d.ncrng[i];
+    A.q = qof(d.quat[i]);
+    A.he = v3of(d.ext[i]);
+    A.dom = a.wp[a.bw[i]].dom;
+    return A;
+}
+
+__device__ __forceinline__ bool cull_keep(const DevWorld& d, const CullA& A, uint32_t j) {
+    const D4 pb = d.pos[j];
+    const uint4 mb = d.meta[j];
+    if (A.invM + pb.w <= 0.0) return false;
+    if (!((A.m.w & (1u << (mb.z & 31u))) && (mb.w & (1u << (A.m.z & 31u))))) return false;
+    for (uint32_t k = 0; k < A.nr.y; ++k)
+        if (d.nc[A.nr.x + k] == j) return false;
+    if ((A.m.y | mb.y) & NE_BODY_SENSOR) return false;
+    const int sa = (int)A.m.x, sb = (int)mb.x;
+    if (sa == SH_PLANE && sb == SH_PLANE) return false;
+    if (sa == SH_PLANE || sb == SH_PLANE) return true;
+    // Bounding spheres about the centres (nearest image).
+    const double rb = d.inert[j].w;
+    const V3 dd = min_image(A.dom, mk(pb.x - A.x.x, pb.y - A.x.y, pb.z - A.x.z));
+    const double r = (A.r + rb) * (1.0 + 1e-9) + 1e-9;
+    if (norm2(dd) > r * r) return false;
+    // Box vs bounding sphere: distance from the sphere centre to the box.
+    if (sa == SH_BOX || sb == SH_BOX) {
+        const bool boxA = (sa == SH_BOX);
+        const double rs = boxA ? rb : A.r;
+        const V3 rel = boxA ? dd : -dd;     // other centre relative to the box centre
+        const Q qb = boxA ? A.q : qof(d.quat[j]);
+        const V3 he = boxA ? A.he : v3of(d.ext[j]);
+        const V3 l = inv_rotate(qb, rel);
+        const double ex = fmax(fabs(l.x) - he.x, 0.0), ey = fmax(fabs(l.y) - he.y, 0.0),
+                     ez = fmax(fabs(l.z) - he.z, 0.0);
+        const double lim = rs * (1.0 + 1e-9) + 1e-9 * (1.0 + norm(he));
+        if (ex * ex + ey * ey + ez * ez > lim * lim) return false;
+    }
+    return true;
+}
+
+// ---- internal grid: cell table, then one pass of filters + cull ------------
+
+constexpr unsigned long long kHashEmpty = ~0ull;
+
+__device__ __forceinline__ uint32_t cell_hash(unsigned long long k, uint32_t mask) {
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return (uint32_t)k & mask;
+}
+
+__global__ void __launch_bounds__(kT) k_hash_clear(StepArgs a) {
+    if (a.d.ctl->abort) return;
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h < a.d.hsize) a.d.hkey[h] = kHashEmpty;
+}
+
+// Run starts of the sorted cell keys (the run of sentinel keys included, so
+// every run has an end), and each body's bounding sphere in sorted order, so
+// the members of a cell are contiguous for the cull.
+__global__ void __launch_bounds__(kT) k_cell_flags(StepArgs a, int kb) {
+    if (a.d.ctl->abort) return;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
+    const DevWorld& d = a.d;
+    const unsigned long long* key = d.key[kb];
+    d.cflag[k] = (k == 0 || key[k] != key[k - 1]) ? 1u : 0u;
+    const uint32_t b = d.val[kb][k];
+    const D4 p = d.pos[b];
+    d.srec[k] = D4{p.x, p.y, p.z, d.inert[b].w};
+}
+
+// cstart of every run, cstart[runs] = n, and the hash entries of the real
+// cells (keys below the sentinel 1 << total).
+__global__ void __launch_bounds__(kT) k_cell_table(StepArgs a, int kb) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
-    const uint64_t pidx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (pidx >= a.Pcap) return;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
     const DevWorld& d = a.d;
-    uint32_t keep = 0;
-    if (pidx < ctl->P) {
-        const uint32_t i = d.pair_i[pidx], j = d.pair_j[pidx];
-        const D4 pa = d.pos[i], pb = d.pos[j];
-        const uint4 ma = d.meta[i], mb = d.meta[j];
-        keep = 1;
-        if (pa.w + pb.w <= 0.0) keep = 0;
-        if (!((ma.w & (1u << (mb.z & 31u))) && (mb.w & (1u << (ma.z & 31u))))) keep = 0;
-        if (keep) {
-            const uint2 nr = d.ncrng[i];
-            for (uint32_t k = 0; k < nr.y; ++k)
-                if (d.nc[nr.x + k] == j) { keep = 0; break; }
+    const uint32_t r = d.crun[k];
+    if (k + 1 == a.n) d.cstart[r + d.cflag[k]] = a.n;
+    if (!d.cflag[k]) return;
+    d.cstart[r] = k;
+    const unsigned long long key = d.key[kb][k];
+    const int total = a.world_bits + (int)ctl->local_bits;
+    if (key >= (1ull << total)) return;
+    const uint32_t mask = d.hsize - 1;
+    uint32_t h = cell_hash(key, mask);
+    for (uint32_t probe = 0; probe < d.hsize; ++probe) {
+        const unsigned long long prev = atomicCAS(&d.hkey[h], kHashEmpty, key);
+        if (prev == kHashEmpty) {
+            d.hval[h] = r;
+            return;
         }
-        if ((ma.y | mb.y) & NE_BODY_SENSOR) keep = 0;
-        const int sa = (int)ma.x, sb = (int)mb.x;
-        if (keep && sa == SH_PLANE && sb == SH_PLANE) keep = 0;
-        if (keep && sa != SH_PLANE && sb != SH_PLANE) {
-            // Bounding spheres about the centres (nearest image).
-            const double ra = d.inert[i].w, rb = d.inert[j].w;
-            const V3 dd = min_image(a.wp[a.bw[i]].dom, mk(pb.x - pa.x, pb.y - pa.y, pb.z - pa.z));
-            const double r = (ra + rb) * (1.0 + 1e-9) + 1e-9;
-            if (norm2(dd) > r * r) keep = 0;
-            // Box vs bounding sphere: distance from the sphere centre to the box.
-            if (keep && (sa == SH_BOX || sb == SH_BOX)) {
-                const bool boxA = (sa == SH_BOX);
-                const uint32_t bi = boxA ? i : j;
-                const double rs = boxA ? rb : ra;
-                const V3 rel = boxA ? dd : -dd;     // other centre relative to the box centre
-                const Q qb = qof(d.quat[bi]);
-                const V3 he = v3of(d.ext[bi]);
-                const V3 l = inv_rotate(qb, rel);
-                const double ex = fmax(fabs(l.x) - he.x, 0.0), ey = fmax(fabs(l.y) - he.y, 0.0),
-                             ez = fmax(fabs(l.z) - he.z, 0.0);
-                const double lim = rs * (1.0 + 1e-9) + 1e-9 * (1.0 + norm(he));
-                if (ex * ex + ey * ey + ez * ez > lim * lim) keep = 0;
+        h = (h + 1) & mask;
+    }
+}
+
+// Sorted positions [lo, hi) of the bodies in cell `key` (empty if none).
+__device__ __forceinline__ void cell_range(const DevWorld& d, unsigned long long key, uint32_t& lo, uint32_t& hi) {
+    lo = hi = 0;
+    if (key == kNoCell) return;
+    const uint32_t mask = d.hsize - 1;
+    uint32_t h = cell_hash(key, mask);
+    for (uint32_t probe = 0; probe < d.hsize; ++probe) {
+        const unsigned long long k = d.hkey[h];
+        if (k == key) {
+            const uint32_t r = d.hval[h];
+            lo = d.cstart[r];
+            hi = d.cstart[r + 1];
+            return;
+        }
+        if (k == kHashEmpty) return;
+        h = (h + 1) & mask;
+    }
+}
+
+// warp_runs with the neighbour cells found through the cell table.
+__device__ __forceinline__ Runs warp_runs_table(const StepArgs& a, const WorldP& W, const GridSel& G,
+                                                const KeyLayout& L, uint32_t i, const D4& p, int kb,
+                                                uint32_t* lo_s, uint32_t* len_s, uint32_t* ex_s) {
+    const int lane = threadIdx.x & 31;
+    const long long cx = cell_of(W, G, p.x, 0), cy = cell_of(W, G, p.y, 1), cz = cell_of(W, G, p.z, 2);
+    const uint32_t* vals = a.d.val[kb];
+    uint32_t rlo = 0, rhi = 0;
+    if (lane < 27) {
+        const int dx = lane / 9 - 1, dy = (lane / 3) % 3 - 1, dz = lane % 3 - 1;
+        unsigned long long k = neighbour_key(L, wrap_cell(W, G, cx + dx, 0), wrap_cell(W, G, cy + dy, 1),
+                                             wrap_cell(W, G, cz + dz, 2));
+        const uint32_t grp = __match_any_sync(0x07ffffffu, k);
+        if (lane == __ffs(grp) - 1) {
+            uint32_t lo, hi;
+            cell_range(a.d, k, lo, hi);
+            rlo = (lo < hi) ? upper_bound_u32(vals, lo, hi, i) : hi;
+            rhi = hi;
+        }
+    } else if (lane == 27) {
+        rlo = upper_bound_u32(G.xl, G.xb, G.xe, i);
+        rhi = G.xe;
+    }
+    const uint32_t len = rhi - rlo;
+    const uint32_t nonempty = __ballot_sync(0xffffffffu, len > 0);
+    const int r = __popc(nonempty & ((1u << lane) - 1u));
+    uint32_t incl = len;
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    Runs R;
+    R.total = __shfl_sync(0xffffffffu, incl, 31);
+    R.nr = __popc(nonempty);
+    R.xl_last = (nonempty >> 27) & 1u;
+    if (len > 0) {
+        lo_s[r] = rlo;
+        len_s[r] = len;
+        ex_s[r] = incl - len;
+    }
+    if (lane == 0) ex_s[R.nr] = R.total;
+    __syncwarp();
+    return R;
+}
+
+// Surviving partners of every body (internal grid), in one pass: each
+// candidate j > i of body i's partner list is tested once with the filters
+// and the cull.  One warp per body.  A body's survivors (at most kSurvBuf;
+// usually a handful) are ranked in shared memory and staged, ascending, at an
+// offset reserved with one atomic per block; bcnt/bstage record count and
+// offset.  A body with more survivors reserves its own space and writes them
+// by a slower exact ranking.  ctl->P accumulates the candidates examined.
+constexpr uint32_t kSurvBuf = 64;
+
+// The bounding-sphere part of cull_keep for a grid candidate, from its
+// sorted record (same arithmetic, so the same decision).
+__device__ __forceinline__ bool sphere_pass(const CullA& A, const D4& s) {
+    const V3 dd = min_image(A.dom, mk(s.x - A.x.x, s.y - A.x.y, s.z - A.x.z));
+    const double r = (A.r + s.w) * (1.0 + 1e-9) + 1e-9;
+    return !(norm2(dd) > r * r);
+}
+
+__global__ void __launch_bounds__(kT, 3) k_surv_gather(StepArgs a, int kb) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    __shared__ uint32_t s_lo[kT / 32][28], s_len[kT / 32][28], s_ex[kT / 32][29];
+    __shared__ uint32_t s_buf[kT / 32][kSurvBuf];
+    __shared__ uint32_t s_cnt[kT / 32], s_cand[kT / 32];
+    __shared__ uint32_t s_base;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const DevWorld& d = a.d;
+    const uint32_t* vals = d.val[kb];
+    uint32_t cnt = 0, cand = 0;
+    bool grid = false;
+    Runs R;
+    R.total = 0; R.nr = 0; R.xl_last = false;
+    CullA A;
+    GridSel G;
+    uint32_t wend = 0;
+    if (i < a.n) {
+        const uint32_t w = a.bw[i];
+        const WorldP& W = a.wp[w];
+        G = grid_sel(a, W, 1);
+        A = cull_self(a, i);
+        wend = W.end;
+        if (G.brute || excluded(A.m, 1)) {
+            cand = W.end - 1 - i;
+            for (uint32_t j0 = i + 1; j0 < W.end; j0 += 32) {
+                const uint32_t j = j0 + lane;
+                const bool k = j < W.end && cull_keep(d, A, j);
+                const uint32_t bal = __ballot_sync(0xffffffffu, k);
+                const uint32_t slot = cnt + __popc(bal & lt);
+                if (k && slot < kSurvBuf) s_buf[wid][slot] = j;
+                cnt += __popc(bal);
+            }
+        } else {
+            grid = true;
+            const KeyLayout L = key_layout(a, w, G, (int)ctl->local_bits);
+            R = warp_runs_table(a, W, G, L, i, d.pos[i], kb, s_lo[wid], s_len[wid], s_ex[wid]);
+            cand = R.total;
+            for (uint32_t e0 = 0; e0 < R.total; e0 += 32) {
+                const uint32_t e = e0 + lane;
+                uint32_t x = 0;
+                bool k = false;
+                if (e < R.total) {
+                    int own;
+                    uint32_t idx;
+                    x = run_candidate(R, s_lo[wid], s_ex[wid], vals, G.xl, e, own, idx);
+                    // Grid members (neither is a plane) fail most often on the
+                    // bounding spheres: test those from the sorted records first.
+                    const bool xl = R.xl_last && own == R.nr - 1;
+                    k = (xl || sphere_pass(A, d.srec[s_lo[wid][own] + idx])) && cull_keep(d, A, x);
+                }
+                const uint32_t bal = __ballot_sync(0xffffffffu, k);
+                const uint32_t slot = cnt + __popc(bal & lt);
+                if (k && slot < kSurvBuf) s_buf[wid][slot] = x;
+                cnt += __popc(bal);
             }
         }
     }
-    d.pflag[pidx] = keep;
+    const bool spill = cnt > kSurvBuf;
+    if (lane == 0) {
+        s_cnt[wid] = spill ? 0u : cnt;
+        s_cand[wid] = cand;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        unsigned long long csum = 0;
+        for (int k = 0; k < kT / 32; ++k) { tot += s_cnt[k]; csum += s_cand[k]; }
+        s_base = tot ? (uint32_t)atomicAdd((unsigned long long*)&ctl->S_stage, (unsigned long long)tot) : 0u;
+        if (csum) atomicAdd((unsigned long long*)&ctl->P, csum);
+    }
+    __syncthreads();
+    if (i >= a.n) return;
+    uint32_t off = s_base;
+    for (int k = 0; k < wid; ++k) off += s_cnt[k];
+    if (!spill) {
+        for (uint32_t t = lane; t < cnt; t += 32) {
+            const uint32_t x = s_buf[wid][t];
+            uint32_t rank = t;   // brute-force and excluded lists are ascending already
+            if (grid) {
+                rank = 0;
+                for (uint32_t u = 0; u < cnt; ++u) rank += (s_buf[wid][u] < x) ? 1u : 0u;
+            }
+            if ((uint64_t)off + rank < a.Scap) d.stage_j[off + rank] = x;
+        }
+    } else {
+        if (lane == 0) off = (uint32_t)atomicAdd((unsigned long long*)&ctl->S_stage, (unsigned long long)cnt);
+        off = __shfl_sync(0xffffffffu, off, 0);
+        if (!grid) {
+            uint32_t out = 0;
+            for (uint32_t j0 = i + 1; j0 < wend && out < cnt; j0 += 32) {
+                const uint32_t j = j0 + lane;
+                const bool k = j < wend && cull_keep(d, A, j);
+                const uint32_t bal = __ballot_sync(0xffffffffu, k);
+                const uint32_t slot = out + __popc(bal & lt);
+                if (k && slot < cnt && (uint64_t)off + slot < a.Scap) d.stage_j[off + slot] = j;
+                out += __popc(bal);
+            }
+        } else {
+            for (uint32_t e = lane; e < R.total; e += 32) {
+                int own;
+                uint32_t idx;
+                const uint32_t x = run_candidate(R, s_lo[wid], s_ex[wid], vals, G.xl, e, own, idx);
+                if (!cull_keep(d, A, x)) continue;
+                uint32_t rank = 0;
+                for (uint32_t u = 0; u < R.total; ++u) {
+                    int o2;
+                    uint32_t i2;
+                    const uint32_t y = run_candidate(R, s_lo[wid], s_ex[wid], vals, G.xl, u, o2, i2);
+                    if (y < x && cull_keep(d, A, y)) ++rank;
+                }
+                if (rank < cnt && (uint64_t)off + rank < a.Scap) d.stage_j[off + rank] = x;
+            }
+        }
+    }
+    if (lane == 0) {
+        d.bcnt[i] = cnt;
+        d.bstage[i] = off;
+    }
 }
 
-__global__ void __launch_bounds__(kT) k_compact(StepArgs a) {
+// Staged partner lists -> the CSR survivor list in body order, which is the
+// reference's sorted pair list (src/world.cpp:496-499) with culled pairs left
+// out.  One warp per body.
+__global__ void __launch_bounds__(kT) k_surv_place(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
-    const uint64_t pidx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ctl->S > a.Scap) {
-        if (pidx == 0) ctl->abort = 1;
+        if (threadIdx.x == 0 && blockIdx.x == 0) ctl->abort = 1;
         return;
     }
-    if (pidx >= a.Pcap) return;
-    if (a.d.pflag[pidx]) a.d.surv[a.d.poff[pidx]] = (uint32_t)pidx;
+    const int lane = threadIdx.x & 31;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= a.n) return;
+    const DevWorld& d = a.d;
+    const uint32_t cnt = d.bcnt[i];
+    if (cnt == 0) return;
+    const uint32_t src = d.bstage[i], dst = d.boff[i];
+    for (uint32_t t = lane; t < cnt; t += 32) {
+        d.si[dst + t] = i;
+        d.sj[dst + t] = d.stage_j[src + t];
+    }
 }
 
 // gatherContacts() for one surviving pair (src/world.cpp:122-129).
@@ -578,14 +892,9 @@ __global__ void __launch_bounds__(128) k_narrowphase(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.Scap) return;
+    if (s >= ctl->S) return;
     const DevWorld& d = a.d;
-    if (s >= ctl->S) {
-        d.ccnt[s] = 0;
-        return;
-    }
-    const uint32_t pidx = d.surv[s];
-    const uint32_t i = d.pair_i[pidx], j = d.pair_j[pidx];
+    const uint32_t i = d.si[s], j = d.sj[s];
     const BodyG A = load_geom(d, i), B = load_geom(d, j);
     EpaScratch S;
     int fl = 0;
@@ -673,8 +982,7 @@ __global__ void __launch_bounds__(kT) k_constraint_build(StepArgs a) {
     const DevWorld& d = a.d;
     const uint32_t cnt = d.ccnt[s];
     if (cnt == 0) return;
-    const uint32_t pidx = d.surv[s];
-    const uint32_t i = d.pair_i[pidx], j = d.pair_j[pidx];
+    const uint32_t i = d.si[s], j = d.sj[s];
     const D4 pa = d.pos[i], pb = d.pos[j];
     const V3 xa = v3of(pa), xb = v3of(pb);
     const V3 va = v3of(d.vel[i]), vb = v3of(d.vel[j]), wa = v3of(d.omg[i]), wb = v3of(d.omg[j]);
@@ -726,19 +1034,17 @@ __global__ void __launch_bounds__(kT) k_constraint_build(StepArgs a) {
 }
 
 // Island label of every constraint (root of its first mutable body) and the
-// identity order; padding entries get label n so they sort last.
+// identity order.  Also publishes 2C, the rank-entry count.
 __global__ void __launch_bounds__(kT) k_island_label(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.Ccap) return;
+    const uint64_t C = ctl->C;
+    if (c == 0) ctl->C2 = 2 * C;
+    if (c >= C) return;
     const DevWorld& d = a.d;
-    uint32_t lab = a.n;
-    if (c < ctl->C) {
-        const uint32_t i = d.ci[c], j = d.cj[c];
-        lab = (d.meta[i].y & kFlagMutable) ? uf_find(d.parent, i) : uf_find(d.parent, j);
-    }
-    d.ilab[0][c] = lab;
+    const uint32_t i = d.ci[c], j = d.cj[c];
+    d.ilab[0][c] = (d.meta[i].y & kFlagMutable) ? uf_find(d.parent, i) : uf_find(d.parent, j);
     d.iord[0][c] = (uint32_t)c;
 }
 
@@ -746,11 +1052,9 @@ __global__ void __launch_bounds__(kT) k_island_mark(StepArgs a, int ib) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= a.Ccap) return;
+    if (k >= ctl->C) return;
     const uint32_t* lab = a.d.ilab[ib];
-    uint32_t f = 0;
-    if (k < ctl->C) f = (k == 0 || lab[k] != lab[k - 1]) ? 1u : 0u;
-    a.d.iflag[k] = f;
+    a.d.iflag[k] = (k == 0 || lab[k] != lab[k - 1]) ? 1u : 0u;
 }
 
 // Island segments.
@@ -767,15 +1071,16 @@ __global__ void __launch_bounds__(kT) k_island_start(StepArgs a) {
 }
 
 // Per-body rank entries: for every contact position p (island order) and each
-// mutable endpoint, key = body, value = 2p + side.  Padding sorts last.
+// mutable endpoint, key = body, value = 2p + side.  Immovable sides get key n
+// and sort last.
 __global__ void __launch_bounds__(kT) k_rank_entries(StepArgs a, int ib) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= a.Ccap) return;
+    if (p >= ctl->C) return;
     const DevWorld& d = a.d;
     uint32_t ka = a.n, kb = a.n;
-    if (p < ctl->C) {
+    {
         const uint32_t c = d.iord[ib][p];
         const uint32_t i = d.ci[c], j = d.cj[c];
         if (d.meta[i].y & kFlagMutable) ka = i;
@@ -793,7 +1098,7 @@ __global__ void __launch_bounds__(kT) k_rank_write(StepArgs a, int rb) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t E = 2 * a.Ccap;
+    const uint64_t E = ctl->C2;
     if (e >= E) return;
     const DevWorld& d = a.d;
     const uint32_t* key = d.rkey[rb];
@@ -818,14 +1123,18 @@ struct BodyS {
     bool mut;
 };
 
+// Mutable solver state (velocities, positions, impulses) goes through
+// solve::ld_state/st_state: plain for one-thread islands, L2-coherent for the
+// team solver, whose consecutive updates of a body may run on different SMs.
+template <bool C>
 __device__ __forceinline__ BodyS load_solver_body(const DevWorld& d, uint32_t i) {
     BodyS b;
-    b.v = v3of(d.vel[i]);
-    b.w = v3of(d.omg[i]);
+    b.v = v3of(solve::ld_state<C>(d.vel + i));
+    b.w = v3of(solve::ld_state<C>(d.omg + i));
     b.q = qof(d.quat[i]);
     const D4 I = d.inert[i];
     b.invI = v3of(I);
-    b.invM = d.pos[i].w;
+    b.invM = d.pos[i].w;   // constant (the correction rewrites pos with the same w)
     b.mut = (d.meta[i].y & kFlagMutable) != 0;
     return b;
 }
@@ -845,97 +1154,101 @@ __device__ __forceinline__ void apply_pair_impulse(BodyS& A, BodyS& B, const V3&
     B.w = B.w - apply_inv_inertia(B.q, B.invI, cross(rb, J));
 }
 
+template <bool C>
 __device__ __forceinline__ void store_solver_body(const DevWorld& d, uint32_t i, const BodyS& b) {
     if (!b.mut) return;   // immovable: +-0 updates leave it unchanged; never written (shared by islands)
-    d.vel[i] = d4of(b.v, 0.0);
-    d.omg[i] = d4of(b.w, 0.0);
+    solve::st_state<C>(d.vel + i, d4of(b.v, 0.0));
+    solve::st_state<C>(d.omg + i, d4of(b.w, 0.0));
 }
 
-// Warm-start application of one contact (src/world.cpp:560-567).
-__device__ __forceinline__ void warm_item(const DevWorld& d, uint32_t c) {
-    const double nImp = d.con_imp[c].x;
-    if (nImp == 0.0) return;
-    const uint32_t i = d.ci[c], j = d.cj[c];
-    BodyS A = load_solver_body(d, i), B = load_solver_body(d, j);
-    const V3 n = v3of(d.con_n[c]), rA = v3of(d.con_ra[c]), rB = v3of(d.con_rb[c]);
-    apply_pair_impulse(A, B, rA, rB, n * nImp);
-    store_solver_body(d, i, A);
-    store_solver_body(d, j, B);
-}
-
-// One sequential-impulse update of one contact (src/world.cpp:575-610).  Kn
-// is the effMass along n computed once at constraint build: the reference
-// recomputes it every sweep from the same (unchanged) operands, so the value
-// is identical.
-__device__ __forceinline__ void sweep_item(const DevWorld& d, uint32_t c) {
-    const uint32_t i = d.ci[c], j = d.cj[c];
-    BodyS A = load_solver_body(d, i), B = load_solver_body(d, j);
-    const D4 cn = d.con_n[c], ra4 = d.con_ra[c], rb4 = d.con_rb[c];
-    const V3 n = v3of(cn), rA = v3of(ra4), rB = v3of(rb4);
-    const double restBias = ra4.w, mu = rb4.w;
-    const double Kn = d.con_kn[c];
-    double2 imp = d.con_imp[c];
-    const V3 vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
-    const double vn = dot(vc, n);
-    if (Kn > 1e-18) {
-        double dj = (restBias - vn) / Kn;
-        const double old = imp.x;
-        imp.x = (old + dj > 0.0) ? old + dj : 0.0;
-        dj = imp.x - old;
-        apply_pair_impulse(A, B, rA, rB, n * dj);
+template <bool C>
+struct ItemsF64 {
+    // Warm-start application of one contact (src/world.cpp:560-567).
+    static __device__ __forceinline__ void warm(const DevWorld& d, uint32_t c) {
+        const double nImp = solve::ld_state<C>(d.con_imp + c).x;
+        if (nImp == 0.0) return;
+        const uint32_t i = d.ci[c], j = d.cj[c];
+        BodyS A = load_solver_body<C>(d, i), B = load_solver_body<C>(d, j);
+        const V3 n = v3of(d.con_n[c]), rA = v3of(d.con_ra[c]), rB = v3of(d.con_rb[c]);
+        apply_pair_impulse(A, B, rA, rB, n * nImp);
+        store_solver_body<C>(d, i, A);
+        store_solver_body<C>(d, j, B);
     }
-    if (mu > 0.0 && imp.x > 0.0) {
-        const V3 vc2 = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
-        const V3 vt = vc2 - n * dot(vc2, n);
-        const double vtl = norm(vt);
-        if (vtl > 1e-12) {
-            const V3 tg = vt / vtl;
-            const double Kt = eff_mass(A, B, rA, rB, tg);
-            if (Kt > 1e-18) {
-                double djt = -vtl / Kt;
-                const double maxF = mu * imp.x;
-                const double old = imp.y;
-                const double sum = old + djt;
-                imp.y = (sum < -maxF) ? -maxF : (sum > maxF ? maxF : sum);
-                djt = imp.y - old;
-                apply_pair_impulse(A, B, rA, rB, tg * djt);
+
+    // One sequential-impulse update of one contact (src/world.cpp:575-610).
+    // Kn is the effMass along n computed once at constraint build: the
+    // reference recomputes it every sweep from the same (unchanged) operands,
+    // so the value is identical.
+    static __device__ __forceinline__ void sweep(const DevWorld& d, uint32_t c) {
+        const uint32_t i = d.ci[c], j = d.cj[c];
+        BodyS A = load_solver_body<C>(d, i), B = load_solver_body<C>(d, j);
+        const D4 cn = d.con_n[c], ra4 = d.con_ra[c], rb4 = d.con_rb[c];
+        const V3 n = v3of(cn), rA = v3of(ra4), rB = v3of(rb4);
+        const double restBias = ra4.w, mu = rb4.w;
+        const double Kn = d.con_kn[c];
+        double2 imp = solve::ld_state<C>(d.con_imp + c);
+        const V3 vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+        const double vn = dot(vc, n);
+        if (Kn > 1e-18) {
+            double dj = (restBias - vn) / Kn;
+            const double old = imp.x;
+            imp.x = (old + dj > 0.0) ? old + dj : 0.0;
+            dj = imp.x - old;
+            apply_pair_impulse(A, B, rA, rB, n * dj);
+        }
+        if (mu > 0.0 && imp.x > 0.0) {
+            const V3 vc2 = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+            const V3 vt = vc2 - n * dot(vc2, n);
+            const double vtl = norm(vt);
+            if (vtl > 1e-12) {
+                const V3 tg = vt / vtl;
+                const double Kt = eff_mass(A, B, rA, rB, tg);
+                if (Kt > 1e-18) {
+                    double djt = -vtl / Kt;
+                    const double maxF = mu * imp.x;
+                    const double old = imp.y;
+                    const double sum = old + djt;
+                    imp.y = (sum < -maxF) ? -maxF : (sum > maxF ? maxF : sum);
+                    djt = imp.y - old;
+                    apply_pair_impulse(A, B, rA, rB, tg * djt);
+                }
             }
         }
+        solve::st_state<C>(d.con_imp + c, imp);
+        store_solver_body<C>(d, i, A);
+        store_solver_body<C>(d, j, B);
     }
-    d.con_imp[c] = imp;
-    store_solver_body(d, i, A);
-    store_solver_body(d, j, B);
-}
 
-// correctPenetration (src/contact.hpp:78-85) and the warm-cache store value.
-__device__ __forceinline__ void correct_item(const DevWorld& d, uint32_t c, double beta, double* wimp_out) {
-    const uint32_t i = d.ci[c], j = d.cj[c];
-    const D4 pa = d.pos[i], pb = d.pos[j];
-    const double invSum = pa.w + pb.w;
-    const D4 cn = d.con_n[c];
-    const double overlap = cn.w;
-    if (!(invSum <= 0.0 || overlap <= 0.0)) {
-        const V3 corr = v3of(cn) * (beta * overlap / invSum);
-        if (d.meta[i].y & kFlagMutable) d.pos[i] = d4of(v3of(pa) + corr * pa.w, pa.w);
-        if (d.meta[j].y & kFlagMutable) d.pos[j] = d4of(v3of(pb) - corr * pb.w, pb.w);
-    }
-    if (wimp_out) wimp_out[c] = d.con_imp[c].x;
-}
-
-struct ItemsF64 {
-    static __device__ __forceinline__ void warm(const DevWorld& d, uint32_t c) { warm_item(d, c); }
-    static __device__ __forceinline__ void sweep(const DevWorld& d, uint32_t c) { sweep_item(d, c); }
-    static __device__ __forceinline__ void correct(const DevWorld& d, uint32_t c, double beta, double* wout) {
-        correct_item(d, c, beta, wout);
+    // correctPenetration (src/contact.hpp:78-85) and the warm-cache store value.
+    static __device__ __forceinline__ void correct(const DevWorld& d, uint32_t c, double beta, double* wimp_out) {
+        const uint32_t i = d.ci[c], j = d.cj[c];
+        const D4 pa = solve::ld_state<C>(d.pos + i), pb = solve::ld_state<C>(d.pos + j);
+        const double invSum = pa.w + pb.w;
+        const D4 cn = d.con_n[c];
+        const double overlap = cn.w;
+        if (!(invSum <= 0.0 || overlap <= 0.0)) {
+            const V3 corr = v3of(cn) * (beta * overlap / invSum);
+            if (d.meta[i].y & kFlagMutable) solve::st_state<C>(d.pos + i, d4of(v3of(pa) + corr * pa.w, pa.w));
+            if (d.meta[j].y & kFlagMutable) solve::st_state<C>(d.pos + j, d4of(v3of(pb) - corr * pb.w, pb.w));
+        }
+        if (wimp_out) wimp_out[c] = solve::ld_state<C>(d.con_imp + c).x;
     }
 };
 
 __global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
-    solve::island_solve_small<ItemsF64>(a, ib);
+    solve::island_solve_small<ItemsF64<false>>(a, ib);
 }
 
+__global__ void __launch_bounds__(solve::kPlanThreads) k_big_plan(StepArgs a, uint32_t G) { solve::big_plan(a, G); }
+
+__global__ void __launch_bounds__(256) k_big_init(StepArgs a, int ib) { solve::big_init(a, ib); }
+
 __global__ void __launch_bounds__(solve::kMaxBigThreads) k_island_solve_big(StepArgs a, int ib, int rb) {
-    solve::island_solve_big<ItemsF64>(a, ib, rb);
+    solve::island_solve_team<ItemsF64<true>>(a, ib, rb);
+}
+
+__global__ void __launch_bounds__(solve::kMaxBigThreads) k_island_solve_local(StepArgs a, int ib, int rb) {
+    solve::island_solve_local<ItemsF64<false>>(a, ib, rb);
 }
 
 // wrapPositions() / applyWalls() (src/world.cpp:698-702, 635-657).
@@ -991,6 +1304,13 @@ inline uint32_t blocks_for(uint64_t n, int t) { return (uint32_t)((n + t - 1) / 
 
 }  // namespace
 
+// Teams and dataflow state of the big islands (both precisions).
+void launch_big_prep(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launches) {
+    k_big_plan<<<1, solve::kPlanThreads, 0, st>>>(a, (uint32_t)(a.num_sms * a.big_ctas_per_sm));
+    k_big_init<<<a.num_sms * 2, 256, 0, st>>>(a, ib);
+    *launches += 2;
+}
+
 // Enqueue one step.  The host reads ctl afterwards to learn whether it must
 // be re-run with larger buffers.
 void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEvent_t* ev) {
@@ -1020,19 +1340,26 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
             uint32_t* vals[2] = {d.val[0], d.val[1]};
             kb = radix_sort_u64(keys, vals, a.n, a.key_bits, d.hist, d.tsum, ctl, st, launches);
         }
-        k_pair_count<<<blocks_for(a.n, kT), kT, 0, st>>>(a, kb, fast); ++L;
-        uint64_t* total = fast ? &ctl->P : &ctl->P_ref;
-        scan_u32(d.bcnt, d.boff, a.n, d.tsum, total, ctl, st, launches);
-        k_pair_emit<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a, kb, fast, fast ? d.pair_i : d.rec_i,
-                                                                      fast ? d.pair_j : d.rec_j, total,
-                                                                      fast ? a.Pcap : a.Rcap); ++L;
+        if (!fast) {
+            k_pair_count<<<blocks_for(a.n, kT), kT, 0, st>>>(a, kb, 0); ++L;
+            scan_u32(d.bcnt, d.boff, a.n, d.tsum, &ctl->P_ref, ctl, st, launches);
+            k_pair_emit<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a, kb, 0, d.rec_i, d.rec_j, &ctl->P_ref,
+                                                                          a.Rcap); ++L;
+            continue;
+        }
+        // Internal grid: cell table, then the filters and the cull inside
+        // the partner lists.
+        if (a.any_grid) {
+            k_hash_clear<<<blocks_for(d.hsize, kT), kT, 0, st>>>(a); ++L;
+            k_cell_flags<<<blocks_for(a.n, kT), kT, 0, st>>>(a, kb); ++L;
+            scan_u32(d.cflag, d.crun, a.n, d.tsum, &ctl->ncells, ctl, st, launches);
+            k_cell_table<<<blocks_for(a.n, kT), kT, 0, st>>>(a, kb); ++L;
+        }
+        mark(2);
+        k_surv_gather<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a, kb); ++L;
+        scan_u32(d.bcnt, d.boff, a.n, d.tsum, &ctl->S, ctl, st, launches);
+        k_surv_place<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a); ++L;
     }
-
-    mark(2);
-    // Narrowphase on the pairs that survive the filters and the cull.
-    k_pair_cull<<<blocks_for(a.Pcap, kT), kT, 0, st>>>(a); ++L;
-    scan_u32(d.pflag, d.poff, (uint32_t)a.Pcap, d.tsum, &ctl->S, ctl, st, launches);
-    k_compact<<<blocks_for(a.Pcap, kT), kT, 0, st>>>(a); ++L;
     mark(3);
     if (a.f32) {
         launch_narrowphase_f32(a, st, launches);
@@ -1040,7 +1367,7 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
         k_narrowphase<<<blocks_for(a.Scap, 128), 128, 0, st>>>(a); ++L;
     }
     mark(4);
-    scan_u32(d.ccnt, d.coff, (uint32_t)a.Scap, d.tsum, &ctl->C, ctl, st, launches);
+    scan_u32(d.ccnt, d.coff, (uint32_t)a.Scap, d.tsum, &ctl->C, ctl, st, launches, &ctl->S);
     k_constraint_build<<<blocks_for(a.Scap, kT), kT, 0, st>>>(a); ++L;
 
     mark(5);
@@ -1050,22 +1377,28 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
     while ((1ull << lbits) <= (unsigned long long)a.n) ++lbits;
     uint32_t* labs[2] = {d.ilab[0], d.ilab[1]};
     uint32_t* ords[2] = {d.iord[0], d.iord[1]};
-    const int ib = radix_sort_u32(labs, ords, (uint32_t)a.Ccap, lbits, d.hist, d.tsum, ctl, st, launches);
+    const int ib = radix_sort_u32(labs, ords, (uint32_t)a.Ccap, lbits, d.hist, d.tsum, ctl, st, launches, &ctl->C);
     k_island_mark<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a, ib); ++L;
-    scan_u32(d.iflag, d.ioff, (uint32_t)a.Ccap, d.tsum, &ctl->scan_total, ctl, st, launches);
+    scan_u32(d.iflag, d.ioff, (uint32_t)a.Ccap, d.tsum, &ctl->scan_total, ctl, st, launches, &ctl->C);
     k_island_start<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a); ++L;
     // Per-body update ranks for the dataflow solver.
     k_rank_entries<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a, ib); ++L;
     uint32_t* rks[2] = {d.rkey[0], d.rkey[1]};
     uint32_t* rvs[2] = {d.rval[0], d.rval[1]};
-    const int rb = radix_sort_u32(rks, rvs, (uint32_t)(2 * a.Ccap), lbits, d.hist, d.tsum, ctl, st, launches);
+    const int rb = radix_sort_u32(rks, rvs, (uint32_t)(2 * a.Ccap), lbits, d.hist, d.tsum, ctl, st, launches,
+                                  &ctl->C2);
     k_rank_write<<<blocks_for(2 * a.Ccap, kT), kT, 0, st>>>(a, rb); ++L;
     mark(6);
     if (a.f32) {
         launch_solve_f32(a, ib, rb, st, launches);
     } else {
         k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib); ++L;
-        k_island_solve_big<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb); ++L;
+        if (a.big_team_max == 1) {
+            k_island_solve_local<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb); ++L;
+        } else {
+            launch_big_prep(a, ib, st, launches);
+            k_island_solve_big<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb); ++L;
+        }
     }
     mark(7);
     k_boundary<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;

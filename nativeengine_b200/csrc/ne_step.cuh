@@ -44,10 +44,11 @@ struct StepArgs {
     int warm;                // warm starting (one setting for the whole batch)
     int record;              // also build the reference-rule pair list
     int f32;                 // batched FP32 form: FP32 narrowphase, constraints and solve
-    uint64_t Pcap, Scap, Ccap, Rcap;
+    uint64_t Scap, Ccap, Rcap;
     int num_sms;
     int big_threads;         // threads per CTA of the big-island solver (tuned)
     int big_ctas_per_sm;     // CTAs per SM of the big-island solver (tuned)
+    int big_team_max;        // CTAs per big island: 1 = block-local solver, > 1 = team solver (tuned)
 };
 
 // ev: NE_NUM_STAGES + 1 events recorded at the stage boundaries, or nullptr.
@@ -57,6 +58,8 @@ void launch_step(const StepArgs& a, cudaStream_t st, uint64_t* launches, cudaEve
 // the FP64 constraint build writes the FP32 solver records itself.
 void launch_narrowphase_f32(const StepArgs& a, cudaStream_t st, uint64_t* launches);
 void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches);
+// Teams and dataflow state of the big islands (ne_step.cu; both precisions).
+void launch_big_prep(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launches);
 // Convex vertex pool D4 -> F4 (upload time).
 void convert_verts_f32(const D4* src, F4* dst, uint32_t count, cudaStream_t st);
 

@@ -60,14 +60,9 @@ __global__ void __launch_bounds__(128) k_narrowphase_f32(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= a.Scap) return;
+    if (s >= ctl->S) return;
     const DevWorld& d = a.d;
-    if (s >= ctl->S) {
-        d.ccnt[s] = 0;
-        return;
-    }
-    const uint32_t pidx = d.surv[s];
-    const uint32_t i = d.pair_i[pidx], j = d.pair_j[pidx];
+    const uint32_t i = d.si[s], j = d.sj[s];
     const Domain dom = a.wp[a.bw[i]].dom;
     const V3 xi = v3d(d.pos[i]), xj = v3d(d.pos[j]);
     const V3 dij = min_image(dom, xj - xi);
@@ -111,22 +106,24 @@ struct BodyF {
     bool mut;
 };
 
+template <bool C>
 __device__ __forceinline__ BodyF load_body_f32(const DevWorld& d, uint32_t i) {
     BodyF b;
-    const F4 v = d.f_v[i];
+    const F4 v = solve::ld_state<C>(d.f_v + i);
     b.v = v3f(v);
     b.invM = v.w;
-    b.w = v3f(d.f_w[i]);
+    b.w = v3f(solve::ld_state<C>(d.f_w + i));
     b.q = qf(d.f_q[i]);
     b.invI = v3f(d.f_I[i]);
     b.mut = (d.meta[i].y & kFlagMutable) != 0;
     return b;
 }
 
+template <bool C>
 __device__ __forceinline__ void store_body_f32(const DevWorld& d, uint32_t i, const BodyF& b) {
     if (!b.mut) return;   // immovable: shared by islands, never written
-    d.f_v[i] = f4of(b.v, b.invM);
-    d.f_w[i] = f4of(b.w, 0.0f);
+    solve::st_state<C>(d.f_v + i, f4of(b.v, b.invM));
+    solve::st_state<C>(d.f_w + i, f4of(b.w, 0.0f));
 }
 
 // effMass (src/contact.hpp:28-33).
@@ -145,28 +142,29 @@ __device__ __forceinline__ void apply_pair_impulse_f32(BodyF& A, BodyF& B, const
     B.w = B.w - apply_inv_inertia(B.q, B.invI, cross(rb, J));
 }
 
+template <bool C>
 struct ItemsF32 {
     // Warm-start application (src/world.cpp:560-567).
     static __device__ __forceinline__ void warm(const DevWorld& d, uint32_t c) {
-        const double nImp = d.con_imp[c].x;
+        const double nImp = solve::ld_state<C>(d.con_imp + c).x;
         if (nImp == 0.0) return;
         const uint32_t i = d.ci[c], j = d.cj[c];
-        BodyF A = load_body_f32(d, i), B = load_body_f32(d, j);
+        BodyF A = load_body_f32<C>(d, i), B = load_body_f32<C>(d, j);
         apply_pair_impulse_f32(A, B, v3f(d.f_ra[c]), v3f(d.f_rb[c]), v3f(d.f_n[c]) * (float)nImp);
-        store_body_f32(d, i, A);
-        store_body_f32(d, j, B);
+        store_body_f32<C>(d, i, A);
+        store_body_f32<C>(d, j, B);
     }
 
     // One sequential-impulse update (src/world.cpp:575-610).  nImp
     // accumulates in FP64; the velocity change it implies is FP32.
     static __device__ __forceinline__ void sweep(const DevWorld& d, uint32_t c) {
         const uint32_t i = d.ci[c], j = d.cj[c];
-        BodyF A = load_body_f32(d, i), B = load_body_f32(d, j);
+        BodyF A = load_body_f32<C>(d, i), B = load_body_f32<C>(d, j);
         const F4 ra4 = d.f_ra[c], rb4 = d.f_rb[c];
         const V3f n = v3f(d.f_n[c]), rA = v3f(ra4), rB = v3f(rb4);
         const float restBias = ra4.w, mu = rb4.w;
         const float Kn = d.f_kn[c];
-        double2 imp = d.con_imp[c];
+        double2 imp = solve::ld_state<C>(d.con_imp + c);
         const V3f vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
         const float vn = dot(vc, n);
         if (Kn > 1e-18f) {
@@ -194,33 +192,39 @@ struct ItemsF32 {
                 }
             }
         }
-        d.con_imp[c] = imp;
-        store_body_f32(d, i, A);
-        store_body_f32(d, j, B);
+        solve::st_state<C>(d.con_imp + c, imp);
+        store_body_f32<C>(d, i, A);
+        store_body_f32<C>(d, j, B);
     }
 
     // correctPenetration (src/contact.hpp:78-85): FP32 displacement, FP64 pose.
     static __device__ __forceinline__ void correct(const DevWorld& d, uint32_t c, double beta, double* wout) {
         const uint32_t i = d.ci[c], j = d.cj[c];
-        const D4 pa = d.pos[i], pb = d.pos[j];
+        const D4 pa = solve::ld_state<C>(d.pos + i), pb = solve::ld_state<C>(d.pos + j);
         const float invSum = (float)pa.w + (float)pb.w;
         const F4 n4 = d.f_n[c];
         const float overlap = n4.w;
         if (!(invSum <= 0.0f || overlap <= 0.0f)) {
             const V3f corr = v3f(n4) * ((float)beta * overlap / invSum);
-            if (d.meta[i].y & kFlagMutable) d.pos[i] = d4of(v3d(pa) + cvt<double>(corr * (float)pa.w), pa.w);
-            if (d.meta[j].y & kFlagMutable) d.pos[j] = d4of(v3d(pb) - cvt<double>(corr * (float)pb.w), pb.w);
+            if (d.meta[i].y & kFlagMutable)
+                solve::st_state<C>(d.pos + i, d4of(v3d(pa) + cvt<double>(corr * (float)pa.w), pa.w));
+            if (d.meta[j].y & kFlagMutable)
+                solve::st_state<C>(d.pos + j, d4of(v3d(pb) - cvt<double>(corr * (float)pb.w), pb.w));
         }
-        if (wout) wout[c] = d.con_imp[c].x;
+        if (wout) wout[c] = solve::ld_state<C>(d.con_imp + c).x;
     }
 };
 
 __global__ void __launch_bounds__(128) k_island_solve_f32(StepArgs a, int ib) {
-    solve::island_solve_small<ItemsF32>(a, ib);
+    solve::island_solve_small<ItemsF32<false>>(a, ib);
 }
 
 __global__ void __launch_bounds__(solve::kMaxBigThreads) k_island_solve_big_f32(StepArgs a, int ib, int rb) {
-    solve::island_solve_big<ItemsF32>(a, ib, rb);
+    solve::island_solve_team<ItemsF32<true>>(a, ib, rb);
+}
+
+__global__ void __launch_bounds__(solve::kMaxBigThreads) k_island_solve_local_f32(StepArgs a, int ib, int rb) {
+    solve::island_solve_local<ItemsF32<false>>(a, ib, rb);
 }
 
 // Solver velocities back into the FP64 state: v64 += v32 - fl(v64).
@@ -255,7 +259,12 @@ void launch_narrowphase_f32(const StepArgs& a, cudaStream_t st, uint64_t* launch
 
 void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches) {
     k_island_solve_f32<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib);
-    k_island_solve_big_f32<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb);
+    if (a.big_team_max == 1) {
+        k_island_solve_local_f32<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb);
+    } else {
+        launch_big_prep(a, ib, st, launches);
+        k_island_solve_big_f32<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb);
+    }
     k_writeback_f32<<<blocks_for(a.n, kT), kT, 0, st>>>(a);
     *launches += 3;
 }

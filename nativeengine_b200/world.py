@@ -151,10 +151,10 @@ class DeviceWorld:
     def solver_shape(self):
         s = _ffi.NeSolverShape()
         _ffi.check(self._lib.ne_world_get_solver_shape(self._h, C.byref(s)), "ne_world_get_solver_shape")
-        return int(s.threads), int(s.ctas_per_sm)
+        return int(s.threads), int(s.ctas_per_sm), int(s.team_max)
 
-    def set_solver_shape(self, threads: int, ctas_per_sm: int = 1):
-        s = _ffi.NeSolverShape(threads, ctas_per_sm)
+    def set_solver_shape(self, threads: int, ctas_per_sm: int = 1, team_max: int = 1):
+        s = _ffi.NeSolverShape(threads, ctas_per_sm, team_max)
         _ffi.check(self._lib.ne_world_set_solver_shape(self._h, C.byref(s)), "ne_world_set_solver_shape")
 
     def autotune(self, steps: int = 5):
@@ -162,7 +162,7 @@ class DeviceWorld:
         keep the fastest; the state is left as it was."""
         s = _ffi.NeSolverShape()
         _ffi.check(self._lib.ne_world_autotune(self._h, steps, C.byref(s)), "ne_world_autotune")
-        return int(s.threads), int(s.ctas_per_sm)
+        return int(s.threads), int(s.ctas_per_sm), int(s.team_max)
 
     def checkpoint(self) -> "Checkpoint":
         """Device copy of the state and the warm cache (see restore())."""

@@ -128,12 +128,35 @@ def test_autotune_keeps_state_and_results():
     dev_a.step(30)
     dev_b.step(30)
     shape = dev_b.autotune(steps=2)
-    assert shape[0] in (128, 256, 512) and 1 <= shape[1] <= 4
+    assert shape[0] in (128, 256, 512) and 1 <= shape[1] <= 4 and 1 <= shape[2] <= 64
     assert dev_b.solver_shape() == shape
     dev_a.step(4)
     dev_b.step(4)
     a, b = dev_a.state(), dev_b.state()
     for key in ("x", "q", "v", "w"):
         assert np.array_equal(a[key], b[key]), key
+    dev_a.close()
+    dev_b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["f64", "f32"])
+def test_team_solver_matches_block_local(precision):
+    """Big islands solved by teams of CTAs reproduce the one-CTA solver bit for bit."""
+    dev_a, _ = _make("box_pile_216")
+    dev_b, _ = _make("box_pile_216")
+    for dev in (dev_a, dev_b):
+        dev.set_precision(precision)
+    dev_a.set_solver_shape(256, 1, 1)
+    dev_b.set_solver_shape(128, 2, 8)
+    dev_a.step(90)   # settle into one big island
+    dev_b.step(90)
+    for _ in range(3):
+        dev_a.step(10)
+        dev_b.step(10)
+        a, b = dev_a.state(), dev_b.state()
+        for key in ("x", "q", "v", "w"):
+            assert np.array_equal(a[key], b[key]), key
+    assert dev_b.stats()["max_island"] >= 48, "no big island exercised"
     dev_a.close()
     dev_b.close()
