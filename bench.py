@@ -297,6 +297,14 @@ def run_ours(args):
     made = make()
     params, bodies = made[0], made[1]
     begin = made[2] if len(made) > 2 else None
+    n_total = bodies.n
+    if begin is not None and world > 1:
+        # Independent worlds: each rank steps its own contiguous share (by
+        # body count) on its own GPU; nothing crosses ranks during a step.
+        from nativeengine_b200.shard import partition_worlds, slice_bodies
+        w0, w1 = partition_worlds(begin, world)[rank]
+        bodies, begin = slice_bodies(bodies, begin, w0, w1)
+        params = params[w0:w1]
     n = bodies.n
     if begin is None:
         dev = DeviceWorld(params, bodies.copy(), record=False, precision=args.precision)
@@ -360,8 +368,12 @@ def run_ours(args):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         t_dev, t_e2e = float(t[0]), float(t[1])
     K = args.steps
-    value = world * n * K / t_dev
-    e2e_value = world * n * K / t_e2e
+    # Whole-job throughput: replicas each step the full workload; a sharded
+    # batch steps each world once across all ranks.
+    sharded = begin is not None and world > 1
+    work = n_total if sharded else world * n
+    value = work * K / t_dev
+    e2e_value = work * K / t_e2e
 
     if rank == 0:
         peak, peak_kind = load_peaks()
@@ -383,21 +395,24 @@ def run_ours(args):
         step_bytes = 360.0 * n + 16.0 * stats["pairs"] + 272.0 * C_last
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
-            "ms_per_step": t_dev / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": t_dev / K * 1e3, "higher_is_better": True,
+            "scaling": "strong" if sharded else "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "f64" else "f32 (FP64 poses, wrap, warm impulses, EPA tests)",
             "data": "synthetic",
-            "config": {"workload": workload, "bodies": n, "steps_per_run": K, "precision": args.precision,
+            "config": {"workload": workload, "bodies": n_total, "steps_per_run": K, "precision": args.precision,
                        "solver_shape": {"threads": shape[0], "ctas_per_sm": shape[1], "team_max": shape[2],
                                         "autotuned": bool(args.autotune)},
-                       "parallelism": "replicas" if world > 1 else "single world",
+                       "parallelism": (f"dp{world}: worlds sharded by body count, no data-path collective"
+                                       if sharded else ("replicas" if world > 1 else
+                                                        ("batch of worlds" if begin is not None else "single world"))),
                        "l2": "256 MiB buffer rewritten between timed steps (outside the events)"},
             "roofline": {"bound": "hbm", "kernel": "solve (k_island_solve + k_island_solve_big)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "traffic": profile_traffic(C_last),
                          "note": "latency-bound: the exact Gauss-Seidel order is a dependency chain; "
                                  "algorithmic bytes = 144 B/contact + 200 B/body of the last step"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * 32 * n,
-                    "d2h_bytes_per_step": 4 * 32 * n},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * 32 * work,
+                    "d2h_bytes_per_step": 4 * 32 * work},
             "gpu_launches": launches,
             "clocks": clocks,
             "stage_ms_per_step": stage_ms,

@@ -330,3 +330,42 @@ def concat(parts):
     out.nocollide = np.ascontiguousarray(nc, dtype=np.uint32)
     out._c = None
     return out, np.array(begin, dtype=np.uint32)
+
+
+def take_range(bodies: BodyArrays, b0: int, b1: int) -> BodyArrays:
+    """Bodies [b0, b1) as a BodyArrays of their own.  Convex vertex offsets are
+    rebased onto the copied vertices and noCollide partners onto b0 (partners
+    must lie inside the range, as they do for whole worlds of a batch)."""
+    out = BodyArrays.__new__(BodyArrays)
+    out.n = b1 - b0
+    per_body = ("x", "q", "v", "w", "force", "torque", "inv_mass", "inv_inertia", "shape", "radius",
+                "half_height", "half_extents", "friction", "restitution", "linear_damping", "angular_damping",
+                "gravity_scale", "layer", "mask", "flags", "vert_count", "nocollide_count")
+    for k in per_body:
+        setattr(out, k, np.ascontiguousarray(getattr(bodies, k)[b0:b1]))
+    vo, verts, vbase = [], [], 0
+    no, ncl, nbase = [], [], 0
+    for i in range(b0, b1):
+        c = int(bodies.vert_count[i])
+        o = int(bodies.vert_offset[i])
+        vo.append(vbase if c else 0)
+        if c:
+            verts.append(bodies.verts[o:o + c])
+            vbase += c
+        k = int(bodies.nocollide_count[i])
+        s = int(bodies.nocollide_offset[i])
+        no.append(nbase)
+        if k:
+            part = bodies.nocollide[s:s + k].astype(np.int64) - b0
+            if np.any(part < 0) or np.any(part >= out.n):
+                raise ValueError("a noCollide partner lies outside the range")
+            ncl.append(part)
+            nbase += k
+    out.vert_offset = np.array(vo, dtype=np.uint32)
+    out.n_verts = vbase
+    out.verts = np.ascontiguousarray(np.concatenate(verts) if vbase else np.zeros((1, 3)), dtype=np.float64)
+    out.nocollide_offset = np.array(no, dtype=np.uint32)
+    out.n_nocollide = nbase
+    out.nocollide = np.ascontiguousarray(np.concatenate(ncl) if nbase else np.zeros(1), dtype=np.uint32)
+    out._c = None
+    return out
