@@ -282,6 +282,71 @@ def run_reference(args):
     return 0
 
 
+def fp32_one_step_error(dev):
+    """One step from one device checkpoint in FP64 and in FP32, per-body
+    errors |x32-x64|/max(|x64|,1), |q32-q64|, |v32-v64|/max(|v64|,1),
+    |w32-w64|/max(|w64|,1) (max and upper quantiles).  Beside them, the same
+    statistics for FP64 against FP64 with the velocities perturbed by 1e-12
+    relative: the step is discontinuous where the reference's own contact
+    decisions flip (manifold reference face, slop cut, contact on/off), so
+    that baseline bounds what any precision can reach at the max."""
+    import numpy as np
+
+    def stats(a, b):
+        out = {}
+        for k, floor in (("x", 1.0), ("v", 1.0), ("w", 1.0)):
+            d = np.linalg.norm(b[k] - a[k], axis=1) / np.maximum(np.linalg.norm(a[k], axis=1), floor)
+            out[k] = {"max": float(d.max()), "p999": float(np.quantile(d, 0.999)), "p99": float(np.quantile(d, 0.99))}
+        out["q"] = {"max": float(np.linalg.norm(b["q"] - a["q"], axis=1).max())}
+        return out
+
+    with dev.checkpoint() as ck:
+        s0 = dev.state()
+        dev.set_precision("f64")
+        dev.step(1)
+        a = dev.state()
+        dev.restore(ck)
+        dev.upload_state(v=s0["v"] * (1.0 + 1e-12), w=s0["w"] * (1.0 + 1e-12))
+        dev.step(1)
+        c = dev.state()
+        dev.restore(ck)
+        dev.set_precision("f32")
+        dev.step(1)
+        b = dev.state()
+        dev.restore(ck)
+    return {"fp32_vs_fp64": stats(a, b), "fp64_vs_fp64_perturbed_1e-12": stats(a, c),
+            "definition": "one step from the same checkpoint; x, v, w relative to max(|.|, 1); q absolute"}
+
+
+def plain_per_world(params, bodies, begin, steps: int, sample: int = 64):
+    """The plain FP64 path on the batch's worlds one at a time (one
+    single-world handle each, as a user of the reference's World API steps
+    them): device time of `steps` steps for a seeded sample of worlds,
+    extrapolated to the whole batch by body count."""
+    import numpy as np
+    import torch
+    from nativeengine_b200 import DeviceWorld
+    from nativeengine_b200.shard import slice_bodies
+    rng = np.random.default_rng(5)
+    nw = len(begin) - 1
+    pick = sorted(rng.choice(nw, size=min(sample, nw), replace=False).tolist())
+    t_total, b_total = 0.0, 0
+    for w in pick:
+        part, _ = slice_bodies(bodies, begin, w, w + 1)
+        dev = DeviceWorld(params[w], part, record=False)
+        dev.step(2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev.step(steps)
+        torch.cuda.synchronize()
+        t_total += time.perf_counter() - t0
+        b_total += part.n
+        dev.close()
+    rate = b_total * steps / t_total
+    return {"value": rate, "unit": UNIT, "sample": f"{len(pick)} of {nw} worlds, {steps} steps each, "
+            f"one single-world handle per world, FP64, wall clock around synchronised steps"}
+
+
 def run_ours(args):
     import torch
 
@@ -344,7 +409,7 @@ def run_ours(args):
                 dev.step(1)
                 launches += dev.launch_count()
                 if host_io:
-                    st = dev.state()
+                    st = dev.state(out=st)
                 ev1[k].record(stream)
                 flush.zero_()
         barrier()
@@ -360,6 +425,7 @@ def run_ours(args):
     stats = dev.stats()
     dev.profile(False)
     ms_e2e, _ = timed_run(host_io=True)
+    fp32_err = fp32_one_step_error(dev) if args.precision == "f32" else None
 
     t_dev = sum(ms_dev) / 1e3
     t_e2e = sum(ms_e2e) / 1e3
@@ -422,6 +488,10 @@ def run_ours(args):
             "step_roofline": {"algorithmic_bytes_last_step": step_bytes,
                               "achieved_gbs_mean": step_bytes / (t_dev / K) / 1e9},
         }
+        if fp32_err is not None:
+            line["fp32_vs_fp64"] = fp32_err
+        if begin is not None and world == 1 and not args.no_cpu_baseline:
+            line["plain_path_per_world"] = plain_per_world(params, bodies, begin, steps=20)
         if world == 1 and not args.no_cpu_baseline:
             if begin is None:
                 line["cpu_baseline"] = cpu_baseline_reference(args.config, params, bodies)

@@ -233,12 +233,13 @@ int ne_world_islands(NeWorld* world, uint32_t* label, uint32_t n);
 /* Arithmetic precision of the narrowphase and the contact solve.  No
  * counterpart in the reference (which is FP64 throughout).
  *   NE_PRECISION_F64  the default: bit-exact with the reference.
- *   NE_PRECISION_F32  the batched FP32 form: support mappings, GJK, analytic
+ *   NE_PRECISION_F32  the batched FP32 form: support mappings, analytic
  *     pairs, box-box clipping and the sequential-impulse solve in FP32 with
  *     FP32 accumulation, in the reference's contact order; FP64 stays for
  *     pose integration, the minimum-image offsets and the wrap, the
- *     accumulated normal impulses (the warm-start cache), EPA's polytope and
- *     its termination tests, and the body state between steps.
+ *     accumulated normal impulses (the warm-start cache), GJK's simplex and
+ *     EPA's polytope arithmetic with their near-degenerate containment and
+ *     termination tests, and the body state between steps.
  * Takes effect from the next step; may be changed at any time. */
 #define NE_PRECISION_F64 0
 #define NE_PRECISION_F32 1

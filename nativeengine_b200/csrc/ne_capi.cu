@@ -9,6 +9,7 @@
 // runs the step again -- so growth never changes the result, and steady-state
 // steps cost one small device->host read of the control block.
 #include <algorithm>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -92,8 +93,8 @@ struct NeWorld {
     size_t nverts_alloc = 0, nnc_alloc = 0, nplanes_alloc = 0;
     std::vector<double> h_invmass;   // for upload_state packing
     std::vector<neb::D4> stage;      // host packing buffer (uploads)
-    neb::D4* pinned = nullptr;       // page-locked staging for per-step state traffic
-    size_t pinned_cap = 0;
+    double* pinned = nullptr;        // page-locked staging for per-step state traffic (host layout)
+    size_t pinned_cap = 0;           // doubles
     NeStepStats stats{};
     uint64_t launches = 0;
     bool has_bodies = false;
@@ -462,7 +463,7 @@ int ne_world_destroy(NeWorld* w) {
     free_surv_arrays(w);
     free_con_arrays(w);
     neb::DevWorld& d = w->d;
-    dfree(d.verts); dfree(d.nc); dfree(d.planes);
+    dfree(d.verts); dfree(d.nc); dfree(d.planes); dfree(d.io);
     for (int b = 0; b < 2; ++b) { dfree(d.wkey[b]); dfree(d.wimp[b]); }
     dfree(d.hist); dfree(d.tsum); dfree(d.ctl);
     dfree(w->d_wp); dfree(w->d_bw); dfree(w->d_cext); dfree(d.xlist); dfree(d.rec_i); dfree(d.rec_j);
@@ -702,15 +703,40 @@ int ne_world_upload_batch(NeWorld* w, const NeWorldParams* params, uint32_t nwor
 // Pinned host staging for per-step state traffic: 6 records per body
 // (pos, quat, vel, omg, frc, trq), so each transfer is one async copy per
 // array straight from page-locked memory.
-static int ensure_pinned(NeWorld* w) {
-    const size_t need = (size_t)6 * (w->n ? w->n : 1);
-    if (w->pinned_cap >= need) return NE_OK;
+// Page-locked host staging and a device block, both in the C-ABI's host
+// layout (x[3n] | q[4n] | v[3n] | w[3n] | force[3n] | torque[3n]): a state
+// transfer is one copy each way, and kernels scatter / gather the records.
+static int ensure_io(NeWorld* w) {
+    const size_t need = (size_t)19 * (w->n ? w->n : 1);   // doubles
+    if (w->pinned_cap >= need && w->d.io) return NE_OK;
     if (w->pinned) cudaFreeHost(w->pinned);
     w->pinned = nullptr;
     w->pinned_cap = 0;
-    NE_CUDA_TRY(cudaMallocHost((void**)&w->pinned, need * sizeof(neb::D4)));
+    dfree(w->d.io);
+    NE_CUDA_TRY(cudaMallocHost((void**)&w->pinned, need * sizeof(double)));
     w->pinned_cap = need;
+    int rc;
+    if ((rc = dalloc(&w->d.io, need))) return rc;
     return NE_OK;
+}
+
+// memcpy split over a few threads: one thread does not saturate the host
+// memory bandwidth for the ~100 MB a large batch moves per step.
+static void par_copy(void* dst, const void* src, size_t bytes) {
+    const size_t kChunk = (size_t)8 << 20;
+    const unsigned nt = (unsigned)std::min<size_t>(8, bytes / kChunk);
+    if (nt < 2) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    std::vector<std::thread> th;
+    const size_t per = (bytes + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; ++t) {
+        const size_t b0 = t * per, b1 = std::min(bytes, b0 + per);
+        if (b0 >= b1) break;
+        th.emplace_back([=] { std::memcpy((char*)dst + b0, (const char*)src + b0, b1 - b0); });
+    }
+    for (auto& t : th) t.join();
 }
 
 int ne_world_upload_state(NeWorld* w, const double* x, const double* q, const double* v, const double* wv) {
@@ -718,30 +744,24 @@ int ne_world_upload_state(NeWorld* w, const double* x, const double* q, const do
     const uint32_t n = w->n;
     if (!n) return NE_OK;
     int rc;
-    if ((rc = ensure_pinned(w))) return rc;
-    neb::D4* st = w->pinned;
-    const size_t bytes = (size_t)n * sizeof(neb::D4);
-    if (x) {
-        neb::D4* s = st;
-        for (uint32_t i = 0; i < n; ++i) s[i] = neb::D4{x[3 * i], x[3 * i + 1], x[3 * i + 2], w->h_invmass[i]};
-        NE_CUDA_TRY(cudaMemcpyAsync(w->d.pos, s, bytes, cudaMemcpyHostToDevice, w->stream));
+    if ((rc = ensure_io(w))) return rc;
+    NE_CUDA_TRY(cudaSetDevice(w->device));
+    double* st = w->pinned;
+    const size_t N = n;
+    const double* src[4] = {x, q, v, wv};
+    const size_t off[4] = {0, 3 * N, 7 * N, 10 * N};
+    const size_t len[4] = {3 * N, 4 * N, 3 * N, 3 * N};
+    uint32_t mask = 0;
+    for (int k = 0; k < 4; ++k) {
+        if (!src[k]) continue;
+        par_copy(st + off[k], src[k], len[k] * sizeof(double));
+        mask |= 1u << k;
     }
-    if (q) {
-        neb::D4* s = st + n;
-        for (uint32_t i = 0; i < n; ++i) s[i] = neb::D4{q[4 * i], q[4 * i + 1], q[4 * i + 2], q[4 * i + 3]};
-        NE_CUDA_TRY(cudaMemcpyAsync(w->d.quat, s, bytes, cudaMemcpyHostToDevice, w->stream));
-    }
-    if (v) {
-        neb::D4* s = st + 2 * (size_t)n;
-        for (uint32_t i = 0; i < n; ++i) s[i] = neb::D4{v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0};
-        NE_CUDA_TRY(cudaMemcpyAsync(w->d.vel, s, bytes, cudaMemcpyHostToDevice, w->stream));
-    }
-    if (wv) {
-        neb::D4* s = st + 3 * (size_t)n;
-        for (uint32_t i = 0; i < n; ++i) s[i] = neb::D4{wv[3 * i], wv[3 * i + 1], wv[3 * i + 2], 0.0};
-        NE_CUDA_TRY(cudaMemcpyAsync(w->d.omg, s, bytes, cudaMemcpyHostToDevice, w->stream));
-    }
-    // The staging buffer is reused by the next call: wait for the copies.
+    if (!mask) return NE_OK;
+    NE_CUDA_TRY(cudaMemcpyAsync(w->d.io, st, 13 * N * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+    neb::launch_unpack_state(w->d, n, w->d.io, mask, w->stream);
+    NE_CUDA_TRY(cudaGetLastError());
+    // The staging buffer is reused by the next call: wait for the copy.
     NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
     return NE_OK;
 }
@@ -752,24 +772,24 @@ int ne_world_download(NeWorld* w, NeBodyArrays* out) {
     const uint32_t n = std::min(w->n, out->n);
     if (!n) return NE_OK;
     int rc;
-    if ((rc = ensure_pinned(w))) return rc;
-    neb::D4* st = w->pinned;
-    const size_t bytes = (size_t)n * sizeof(neb::D4);
-    const neb::D4* src[6] = {w->d.pos, w->d.quat, w->d.vel, w->d.omg, w->d.frc, w->d.trq};
+    if ((rc = ensure_io(w))) return rc;
+    NE_CUDA_TRY(cudaSetDevice(w->device));
+    const size_t N = w->n;
     double* dst[6] = {out->x, out->q, out->v, out->w, out->force, out->torque};
+    const size_t off[6] = {0, 3 * N, 7 * N, 10 * N, 13 * N, 16 * N};
+    const size_t per[6] = {3, 4, 3, 3, 3, 3};
+    uint32_t mask = 0;
+    size_t end = 0;
     for (int k = 0; k < 6; ++k)
-        if (dst[k]) NE_CUDA_TRY(cudaMemcpyAsync(st + (size_t)k * n, src[k], bytes, cudaMemcpyDeviceToHost, w->stream));
+        if (dst[k]) { mask |= 1u << k; end = off[k] + per[k] * N; }
+    if (!mask) return NE_OK;
+    neb::launch_pack_state(w->d, w->n, w->d.io, mask, w->stream);
+    NE_CUDA_TRY(cudaGetLastError());
+    double* st = w->pinned;
+    NE_CUDA_TRY(cudaMemcpyAsync(st, w->d.io, end * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
     NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
-    for (int k = 0; k < 6; ++k) {
-        if (!dst[k]) continue;
-        const neb::D4* s = st + (size_t)k * n;
-        double* o = dst[k];
-        if (k == 1) {
-            for (uint32_t i = 0; i < n; ++i) { o[4 * i] = s[i].x; o[4 * i + 1] = s[i].y; o[4 * i + 2] = s[i].z; o[4 * i + 3] = s[i].w; }
-        } else {
-            for (uint32_t i = 0; i < n; ++i) { o[3 * i] = s[i].x; o[3 * i + 1] = s[i].y; o[3 * i + 2] = s[i].z; }
-        }
-    }
+    for (int k = 0; k < 6; ++k)
+        if (dst[k]) par_copy(dst[k], st + off[k], per[k] * (size_t)n * sizeof(double));
     return NE_OK;
 }
 

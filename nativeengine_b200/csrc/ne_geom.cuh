@@ -9,10 +9,11 @@
 //
 // The routines are templates over the real type R of the body geometry.
 // R = double is the bit-exact path.  R = float is the batched FP32 form: the
-// support mappings, GJK, the analytic pairs and the clipping run in FP32 in a
-// body-relative frame, while EPA's polytope (face normals and distances, the
-// visibility and termination tests, the barycentric witness) stays FP64 over
-// the FP32 support points, which convert to double exactly.
+// support mappings, the analytic pairs and the clipping run in FP32 in a
+// body-relative frame, while the simplex and polytope arithmetic of GJK and
+// EPA (search directions, containment and termination tests, face normals and
+// distances, the barycentric witness) stays FP64 over the FP32 support
+// points, which convert to double exactly.
 #pragma once
 
 #include "ne_math.cuh"
@@ -283,42 +284,46 @@ NE_HD SupVT<R> cso_support(const BodyGT<R>& A, const BodyGT<R>& B, const Vec3<R>
 
 // GJK returning an origin-enclosing tetrahedron (src/epa.hpp:28-64).  The
 // simplex is kept newest-first, as the reference's front-inserting vector.
+// The simplex arithmetic (search directions, region and termination tests) is
+// FP64 over the support points, which convert exactly; only the support
+// mappings run in R.  For R = double this is the reference's arithmetic
+// unchanged; for R = float it keeps the near-degenerate containment tests
+// exact enough that EPA never starts from a tetrahedron that misses the origin.
 template <typename R>
 NE_HD bool gjk_tetra(const BodyGT<R>& A, const BodyGT<R>& B, const Vec3<R>& shift, SupVT<R> tet[4]) {
-    using V = Vec3<R>;
-    V d = mk3<R>(R(1), R(0), R(0));
-    SupVT<R> s = cso_support(A, B, shift, d);
-    if (norm2(sv(s)) < R(1e-24)) { d = mk3<R>(R(0), R(1), R(0)); s = cso_support(A, B, shift, d); }
+    V3 d = mk(1.0, 0.0, 0.0);
+    SupVT<R> s = cso_support(A, B, shift, cvt<R>(d));
+    if (norm2(svd(s)) < 1e-24) { d = mk(0.0, 1.0, 0.0); s = cso_support(A, B, shift, cvt<R>(d)); }
     SupVT<R> W[4];
     int nw = 1;
     W[0] = s;
-    d = -sv(s);
+    d = -svd(s);
     for (int iter = 0; iter < 64; ++iter) {
-        if (norm2(d) < R(1e-24)) d = mk3<R>(R(1), R(0), R(0));
-        SupVT<R> p = cso_support(A, B, shift, d);
-        if (dot(sv(p), d) <= R(1e-12)) return false;
+        if (norm2(d) < 1e-24) d = mk(1.0, 0.0, 0.0);
+        SupVT<R> p = cso_support(A, B, shift, cvt<R>(d));
+        if (dot(svd(p), d) <= 1e-12) return false;
         for (int k = nw; k > 0; --k) W[k] = W[k - 1];
         W[0] = p;
         ++nw;
-        const V a = sv(W[0]), ao = -a;
+        const V3 a = svd(W[0]), ao = -a;
         if (nw == 2) {
-            V ab = sv(W[1]) - a;
+            V3 ab = svd(W[1]) - a;
             d = cross(cross(ab, ao), ab);
-            if (norm2(d) < R(1e-24)) d = mk3<R>(ab.y, -ab.x, R(0));
+            if (norm2(d) < 1e-24) d = mk(ab.y, -ab.x, 0.0);
         } else if (nw == 3) {
-            V ab = sv(W[1]) - a, ac = sv(W[2]) - a;
-            V abc = cross(ab, ac);
+            V3 ab = svd(W[1]) - a, ac = svd(W[2]) - a;
+            V3 abc = cross(ab, ac);
             if (dot(abc, ao) > 0) {
                 d = abc;
             } else {
                 SupVT<R> t = W[1]; W[1] = W[2]; W[2] = t;
                 d = -abc;
             }
-            if (norm2(d) < R(1e-24)) return false;
+            if (norm2(d) < 1e-24) return false;
         } else {
-            V b = sv(W[1]), c = sv(W[2]), dd = sv(W[3]);
-            V ab = b - a, ac = c - a, ad = dd - a;
-            V abc = cross(ab, ac), acd = cross(ac, ad), adb = cross(ad, ab);
+            V3 b = svd(W[1]), c = svd(W[2]), dd = svd(W[3]);
+            V3 ab = b - a, ac = c - a, ad = dd - a;
+            V3 abc = cross(ab, ac), acd = cross(ac, ad), adb = cross(ad, ab);
             if (dot(abc, ao) > 0) {
                 nw = 3; d = abc;                                   // {W0, W1, W2}
             } else if (dot(acd, ao) > 0) {

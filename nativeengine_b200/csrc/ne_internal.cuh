@@ -132,6 +132,8 @@ struct DevWorld {
     F4* f_verts;             // convex vertices (body frame)
     F4 *f_n, *f_ra, *f_rb;   // [C] (n, overlap), (rA, restBias), (rB, mu)
     float* f_kn;             // [C] effective mass along n
+    // host-layout state block for per-step transfers (19n doubles, lazily allocated)
+    double* io;
     // scratch
     uint32_t *hist, *tsum;
     Ctl* ctl;

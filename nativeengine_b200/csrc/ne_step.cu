@@ -1302,7 +1302,60 @@ __global__ void k_step_end(StepArgs a) {
 
 inline uint32_t blocks_for(uint64_t n, int t) { return (uint32_t)((n + t - 1) / t); }
 
+// Host-layout state block (the C-ABI's interleaved arrays, back to back):
+// x[3n] | q[4n] | v[3n] | w[3n] | force[3n] | torque[3n].  mask bit k selects
+// array k.  Unpacking keeps each record's fourth word (invMass in pos).
+__global__ void __launch_bounds__(kT) k_unpack_state(DevWorld d, uint32_t n, const double* __restrict__ io,
+                                                     uint32_t mask) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t N = n;
+    if (mask & 1u) {
+        const double* x = io + 3 * (size_t)i;
+        d.pos[i] = D4{x[0], x[1], x[2], d.pos[i].w};
+    }
+    if (mask & 2u) {
+        const double* q = io + 3 * N + 4 * (size_t)i;
+        d.quat[i] = D4{q[0], q[1], q[2], q[3]};
+    }
+    if (mask & 4u) {
+        const double* v = io + 7 * N + 3 * (size_t)i;
+        d.vel[i] = D4{v[0], v[1], v[2], 0.0};
+    }
+    if (mask & 8u) {
+        const double* w = io + 10 * N + 3 * (size_t)i;
+        d.omg[i] = D4{w[0], w[1], w[2], 0.0};
+    }
+}
+
+__global__ void __launch_bounds__(kT) k_pack_state(DevWorld d, uint32_t n, double* __restrict__ io, uint32_t mask) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t N = n;
+    const D4* src[6] = {d.pos, d.quat, d.vel, d.omg, d.frc, d.trq};
+    const size_t off[6] = {0, 3 * N, 7 * N, 10 * N, 13 * N, 16 * N};
+    for (int k = 0; k < 6; ++k) {
+        if (!(mask & (1u << k))) continue;
+        const D4 r = src[k][i];
+        if (k == 1) {
+            double* o = io + off[k] + 4 * (size_t)i;
+            o[0] = r.x; o[1] = r.y; o[2] = r.z; o[3] = r.w;
+        } else {
+            double* o = io + off[k] + 3 * (size_t)i;
+            o[0] = r.x; o[1] = r.y; o[2] = r.z;
+        }
+    }
+}
+
 }  // namespace
+
+void launch_unpack_state(const DevWorld& d, uint32_t n, const double* io, uint32_t mask, cudaStream_t st) {
+    if (n) k_unpack_state<<<blocks_for(n, kT), kT, 0, st>>>(d, n, io, mask);
+}
+
+void launch_pack_state(const DevWorld& d, uint32_t n, double* io, uint32_t mask, cudaStream_t st) {
+    if (n) k_pack_state<<<blocks_for(n, kT), kT, 0, st>>>(d, n, io, mask);
+}
 
 // Teams and dataflow state of the big islands (both precisions).
 void launch_big_prep(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launches) {

@@ -60,6 +60,10 @@ void launch_narrowphase_f32(const StepArgs& a, cudaStream_t st, uint64_t* launch
 void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches);
 // Teams and dataflow state of the big islands (ne_step.cu; both precisions).
 void launch_big_prep(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launches);
+// State transfer in the C-ABI's host layout: x[3n] | q[4n] | v[3n] | w[3n] |
+// force[3n] | torque[3n] (mask bit k = array k) to and from the records.
+void launch_unpack_state(const DevWorld& d, uint32_t n, const double* io, uint32_t mask, cudaStream_t st);
+void launch_pack_state(const DevWorld& d, uint32_t n, double* io, uint32_t mask, cudaStream_t st);
 // Convex vertex pool D4 -> F4 (upload time).
 void convert_verts_f32(const D4* src, F4* dst, uint32_t count, cudaStream_t st);
 

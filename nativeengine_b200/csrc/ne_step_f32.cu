@@ -7,9 +7,10 @@
 //                 smaller bounding radius (offset = FP64 minimum image, then
 //                 rounded), so FP32 coordinates stay of the order of the
 //                 bodies' size even in a large or periodic world.  Support
-//                 mappings, GJK, the analytic pairs and the box-box clipping
-//                 run in FP32; EPA's polytope and its termination tests run in
-//                 FP64 over the FP32 support points (ne_geom.cuh).  Contacts
+//                 mappings, the analytic pairs and the box-box clipping run
+//                 in FP32; GJK's simplex and EPA's polytope arithmetic (their
+//                 containment and termination tests) run in FP64 over the
+//                 FP32 support points (ne_geom.cuh).  Contacts
 //                 are stored in the FP64 contact arrays (point = origin +
 //                 FP32 offset, in FP64).
 //   solve         body velocities, lever arms, restitution bias, friction and

@@ -93,12 +93,18 @@ class DeviceWorld:
         _ffi.check(self._lib.ne_world_reset_warm_cache(self._h), "ne_world_reset_warm_cache")
 
     # -- readback ------------------------------------------------------------
-    def state(self, with_forces: bool = False) -> Dict[str, np.ndarray]:
+    def state(self, with_forces: bool = False, out: Optional[Dict[str, np.ndarray]] = None) -> Dict[str, np.ndarray]:
+        """Download x, q, v, w (and force, torque).  `out` reuses caller-owned
+        C-contiguous float64 arrays of the right shapes (no allocation)."""
         n = self.n
-        out = {"x": np.empty((n, 3)), "q": np.empty((n, 4)), "v": np.empty((n, 3)), "w": np.empty((n, 3))}
-        if with_forces:
-            out["force"] = np.empty((n, 3))
-            out["torque"] = np.empty((n, 3))
+        if out is None:
+            out = {"x": np.empty((n, 3)), "q": np.empty((n, 4)), "v": np.empty((n, 3)), "w": np.empty((n, 3))}
+            if with_forces:
+                out["force"] = np.empty((n, 3))
+                out["torque"] = np.empty((n, 3))
+        for k, a in out.items():
+            if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"] or a.shape[0] != n:
+                raise ValueError(f"out[{k!r}] must be a C-contiguous float64 array with {n} rows")
         s = _ffi.NeBodyArrays()
         s.n = n
         for k, a in out.items():

@@ -160,3 +160,19 @@ def test_team_solver_matches_block_local(precision):
     assert dev_b.stats()["max_island"] >= 48, "no big island exercised"
     dev_a.close()
     dev_b.close()
+
+
+@pytest.mark.gpu
+def test_fp32_pose_error_on_a_large_batch_after_fp32_steps():
+    """Batch scale (256 worlds, piles up to ~2k boxes), state reached by FP32
+    stepping: deep piles exercise near-touching GJK/EPA cases in FP32."""
+    params, bodies, begin, _ = scenes.batch_mix(nworlds=256, seed=4)
+    dev = DeviceWorld(params[0], None, record=False, precision="f32")
+    dev.upload_batch(params, bodies, begin)
+    dev.step(100)
+    err = one_step_errors(dev)
+    print(f"batch_256: contacts {err['contacts64']}/{err['contacts32']}  pose {err['x']:.3e}  "
+          f"quat {err['q']:.3e}  vel {err['v']:.3e}")
+    assert err["x"] <= POSE_TOL, err
+    assert err["q"] <= POSE_TOL, err
+    dev.close()
