@@ -67,6 +67,12 @@ def _cfg_batch():
     return params, bodies, begin
 
 
+def _cfg_batch_256():
+    from nativeengine_b200 import scenes
+    params, bodies, begin, kinds = scenes.batch_mix(nworlds=256)
+    return params, bodies, begin
+
+
 def _cfg_granular():
     from nativeengine_b200 import scenes
     return scenes.granular_mix(n=65536, max_attempts=2000)
@@ -81,13 +87,14 @@ CONFIGS = {
                           "(~879k bodies), each a box pile (as box_pile at its size) or a periodic sphere gas "
                           "(as gas_1000 at its size), chosen 50/50 from seed 4; all worlds in one launch "
                           "sequence"),
+    "batch_256": (_cfg_batch_256, "batch_256: the first 256 worlds of the batch_2048 recipe (seed 4; profiling case)"),
     "granular": (_cfg_granular, "granular_65536: periodic mix of spheres/capsules/cylinders/12-point hulls "
                                 "(types by index mod 4), exact-overlap random sequential placement at the "
                                 "densest box that places all bodies (true-volume packing fraction ~0.19), "
                                 "v~N(0,0.5), mu=0.3, e=0.5, g=0, dt=1/60 (seed 3)"),
 }
 # Reference-CPU sample per config: physics steps timed on one host core.
-CPU_SAMPLE_STEPS = {"box_pile": 3, "box_pile_8": 20, "gas": 2000, "granular": 2, "batch": 2}
+CPU_SAMPLE_STEPS = {"box_pile": 3, "box_pile_8": 20, "gas": 2000, "granular": 2, "batch": 2, "batch_256": 2}
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "solve_box_pile_512.md")
 
 
@@ -472,7 +479,7 @@ def run_ours(args):
                                        if sharded else ("replicas" if world > 1 else
                                                         ("batch of worlds" if begin is not None else "single world"))),
                        "l2": "256 MiB buffer rewritten between timed steps (outside the events)"},
-            "roofline": {"bound": "hbm", "kernel": "solve (k_island_solve + k_island_solve_big)",
+            "roofline": {"bound": "hbm", "kernel": "solve (k_island_solve + k_island_solve_local)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "traffic": profile_traffic(C_last),
                          "note": "latency-bound: the exact Gauss-Seidel order is a dependency chain; "
