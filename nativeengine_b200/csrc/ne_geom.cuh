@@ -383,9 +383,11 @@ NE_HD EpaFace epa_make_face(const SupVT<R>* verts, int i, int j, int k) {
 
 // EPA expansion + barycentric witness (src/epa.hpp:71-150).
 // flags |= 1 on a budget overrun, |= 2 when the 64-iteration cap was reached.
+// face_out (optional) receives the final face's three vertices, oriented so
+// that their normal points away from the origin.
 template <typename R>
 NE_HD ContactT<R> epa_contact(const BodyGT<R>& A, const BodyGT<R>& B, const Vec3<R>& shift, const SupVT<R> tet[4],
-                              EpaScratchT<R>& S, int& flags) {
+                              EpaScratchT<R>& S, int& flags, SupVT<R>* face_out = nullptr) {
     SupVT<R>* verts = S.verts;
     EpaFace* faces = S.faces;
     int nv = 4, nf = 4;
@@ -444,6 +446,7 @@ NE_HD ContactT<R> epa_contact(const BodyGT<R>& A, const BodyGT<R>& B, const Vec3
     const SupVT<R>& A0 = verts[best.a];
     const SupVT<R>& B0 = verts[best.b];
     const SupVT<R>& C0 = verts[best.c];
+    if (face_out) { face_out[0] = A0; face_out[1] = B0; face_out[2] = C0; }
     V3 proj = best.n * best.dist;
     V3 a0v = svd(A0);
     V3 v0 = svd(B0) - a0v, v1 = svd(C0) - a0v, v2 = proj - a0v;
@@ -474,17 +477,17 @@ NE_HD Vec3<R> min_image_shift(const BodyGT<R>& A, const BodyGT<R>& B, const Doma
 
 template <typename R>
 NE_HD ContactT<R> convex_contact(const BodyGT<R>& A, const BodyGT<R>& B, const Domain& dom, EpaScratchT<R>& S,
-                                 int& flags) {
+                                 int& flags, SupVT<R>* face_out = nullptr) {
     Vec3<R> shift = min_image_shift(A, B, dom);
     SupVT<R> tet[4];
     if (!gjk_tetra(A, B, shift, tet)) return no_contact_t<R>();
-    return epa_contact(A, B, shift, tet, S, flags);
+    return epa_contact(A, B, shift, tet, S, flags, face_out);
 }
 
 // Narrowphase dispatch (src/detect.hpp:33-77): normal b -> a.
 template <typename R>
 NE_HD ContactT<R> detect_contact(const BodyGT<R>& a, const BodyGT<R>& b, const Domain& dom, EpaScratchT<R>& S,
-                                 int& flags) {
+                                 int& flags, SupVT<R>* face_out = nullptr) {
     if (a.shape == SH_PLANE || b.shape == SH_PLANE) {
         if (a.shape == SH_PLANE && b.shape == SH_PLANE) return no_contact_t<R>();
         const BodyGT<R>& plane = (a.shape == SH_PLANE) ? a : b;
@@ -520,7 +523,7 @@ NE_HD ContactT<R> detect_contact(const BodyGT<R>& a, const BodyGT<R>& b, const D
         if (t.hit) t.normal = -t.normal;
         return t;
     }
-    return convex_contact(a, b, dom, S, flags);
+    return convex_contact(a, b, dom, S, flags, face_out);
 }
 
 // ---- box-box clipping manifold (src/manifold.hpp:16-126) -------------------

@@ -261,3 +261,44 @@ def box_stack(levels=6, friction=0.6, dt=1.0 / 240.0):
         bodies.append(make_box((0.0, 1.0 + i * 2.0, 0.0), (1, 0, 0, 0), (1.0, 1.0, 1.0), 1.0))
     params = default_params(half=1000.0, dt=dt, gravity=(0.0, -10.0, 0.0), restitution=0.0, friction=friction)
     return params, BodyArrays(bodies)
+
+
+# ---- adjoint workload --------------------------------------------------------
+
+def sliding_boxes(grid: int = 8, spacing: float = 1.5, mu: float = 0.5, e: float = 0.25, seed: int = 5,
+                  vsigma: float = 2.0, dt: float = 1.0 / 60.0):
+    """One world of the adjoint workload: a ground plane through the origin
+    (normal +y) and grid x grid boxes of half extent 0.5, density 1, resting at
+    y = 0.5 on a square grid, with horizontal initial velocities N(0, vsigma^2);
+    open boundary, g = -9.81, world friction mu and restitution e (the bodies
+    inherit both)."""
+    rng = _rng(seed)
+    bodies = [make_plane((0.0, 0.0, 0.0), (0.0, 1.0, 0.0))]
+    c = (grid - 1) / 2.0
+    for i in range(grid):
+        for k in range(grid):
+            b = make_box(((i - c) * spacing, 0.5, (k - c) * spacing), (1.0, 0.0, 0.0, 0.0), (0.5, 0.5, 0.5), 1.0)
+            vx, vz = rng.normal(0.0, vsigma, 2)
+            b.v = (float(vx), 0.0, float(vz))
+            bodies.append(b)
+    params = default_params(open_boundary=1, gravity=(0.0, -9.81, 0.0), dt=dt, friction=mu, restitution=e)
+    return params, BodyArrays(bodies)
+
+
+def adjoint_batch(nworlds: int = 512, grid: int = 8, seed: int = 6):
+    """The adjoint workload: nworlds sliding_boxes worlds with per-world
+    friction U[0.2, 0.8] and restitution U[0, 0.5], and loss targets
+    U[-5, 5]^3 per box.  Returns (params_list, BodyArrays, world_begin,
+    targets[n, 3]) (the plane's target row is unused)."""
+    from .bodies import concat
+    rng = _rng(seed)
+    params, parts = [], []
+    for w in range(nworlds):
+        mu = float(rng.uniform(0.2, 0.8))
+        e = float(rng.uniform(0.0, 0.5))
+        p, b = sliding_boxes(grid=grid, mu=mu, e=e, seed=int(rng.integers(1, 2**31 - 1)))
+        params.append(p)
+        parts.append(b)
+    bodies, begin = concat(parts)
+    targets = rng.uniform(-5.0, 5.0, (bodies.n, 3))
+    return params, bodies, begin, targets
