@@ -277,6 +277,39 @@ int ne_world_checkpoint(NeWorld* world, NeCheckpoint** out);
 int ne_world_restore(NeWorld* world, const NeCheckpoint* checkpoint);
 int ne_checkpoint_destroy(NeCheckpoint* checkpoint);
 
+/* Adjoint of step() (stepBackward).  No counterpart in the reference.
+ * Differentiates the trajectory of `nsteps` steps starting from the world's
+ * current state and warm cache: given dL/d(x, v after the last step) in
+ * `final_grad` (either pointer may be NULL for zero), returns dL/d(initial
+ * x, q, v, w), dL/d per-body mass (inverse inertia scaled with the mass, shape
+ * fixed), dL/d per-body inverse mass and inverse inertia, and dL/d per-world
+ * friction and restitution (through the bodies that inherit the world's
+ * values).  Every step is recomputed on the device, one thread per world,
+ * from states checkpointed every `checkpoint_every` steps (0 = one segment);
+ * the contact set, clamps and branches are those of the trajectory, so the
+ * result is the derivative of the piecewise-smooth map on the piece the
+ * trajectory is on.  The world's own state is not changed.  Supported: open
+ * or periodic worlds of planes, boxes and convex hulls (spheres only with
+ * spheres and planes), at most 1024 bodies per world; otherwise
+ * NE_ERR_UNSUPPORTED.  Output pointers may be NULL. */
+typedef struct NeStateGrad {
+    const double* x;        /* [3n] dL/dx after the last step */
+    const double* v;        /* [3n] dL/dv after the last step */
+} NeStateGrad;
+typedef struct NeParamGrad {
+    double* x;              /* [3n] dL/d initial x */
+    double* q;              /* [4n] dL/d initial q (w, x, y, z components) */
+    double* v;              /* [3n] dL/d initial v */
+    double* w;              /* [3n] dL/d initial angular velocity */
+    double* mass;           /* [n] dL/d mass (bodies with invMass > 0; else 0) */
+    double* inv_mass;       /* [n] */
+    double* inv_inertia;    /* [3n] */
+    double* friction;       /* [nworlds] dL/d World::friction */
+    double* restitution;    /* [nworlds] dL/d World::restitution */
+} NeParamGrad;
+int ne_world_step_backward(NeWorld* world, uint32_t nsteps, uint32_t checkpoint_every,
+                           const NeStateGrad* final_grad, NeParamGrad* out);
+
 /* The CUDA stream the world launches on (as a void*; cast to cudaStream_t). */
 int ne_world_stream(const NeWorld* world, void** stream);
 /* Number of kernel launches made by the last ne_world_step call. */

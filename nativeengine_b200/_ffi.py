@@ -92,6 +92,18 @@ class NeSolverShape(C.Structure):
     _fields_ = [("threads", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("team_max", C.c_uint32)]
 
 
+_cdp = C.POINTER(C.c_double)
+
+
+class NeStateGrad(C.Structure):
+    _fields_ = [("x", _cdp), ("v", _cdp)]
+
+
+class NeParamGrad(C.Structure):
+    _fields_ = [("x", _cdp), ("q", _cdp), ("v", _cdp), ("w", _cdp), ("mass", _cdp), ("inv_mass", _cdp),
+                ("inv_inertia", _cdp), ("friction", _cdp), ("restitution", _cdp)]
+
+
 class NeStepStats(C.Structure):
     _fields_ = [
         ("pairs", C.c_uint64), ("survivors", C.c_uint64), ("contacts", C.c_uint64),
@@ -124,6 +136,8 @@ EXPORTS = {
     "ne_world_set_solver_shape": (C.c_int, [C.c_void_p, C.POINTER(NeSolverShape)]),
     "ne_world_get_solver_shape": (C.c_int, [C.c_void_p, C.POINTER(NeSolverShape)]),
     "ne_world_autotune": (C.c_int, [C.c_void_p, C.c_uint32, C.POINTER(NeSolverShape)]),
+    "ne_world_step_backward": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(NeStateGrad),
+                                         C.POINTER(NeParamGrad)]),
     "ne_world_checkpoint": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "ne_world_restore": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ne_checkpoint_destroy": (C.c_int, [C.c_void_p]),

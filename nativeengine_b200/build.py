@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "_lib", "libne_cuda.so")
 OBJDIR = os.path.join(HERE, "_build")
-SOURCES = ["ne_prims.cu", "ne_step.cu", "ne_step_f32.cu", "ne_capi.cu", "ne_noalloc.cu"]
+SOURCES = ["ne_prims.cu", "ne_step.cu", "ne_step_f32.cu", "ne_adjoint.cu", "ne_capi.cu", "ne_noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC"]
 # Per-source contraction setting: off everywhere except the FP32 form.

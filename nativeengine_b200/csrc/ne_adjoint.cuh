@@ -1050,4 +1050,47 @@ NE_HD void bwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w, St* s
 }
 
 }  // namespace adj
+
+// ---- stepBackward launch ----------------------------------------------------------
+
+constexpr uint32_t kAdjMaxBodies = 1024;
+
+// Everything k_adj_world reads and writes (device pointers).  Body-indexed
+// arrays use global body indices; contact-indexed ones give world w the range
+// [coff[w], coff[w] + cap[w]) of CT entries.  Warm-cache slots: 0-1 the
+// running caches, 2 .. 2+nck-1 the checkpoints, 2+nck .. 2+nck+K-1 the
+// recomputed segment; slot s of world w lives at s*CT + coff[w] (counts at
+// s*nworlds + w).
+struct AdjArgs {
+    DevWorld d;
+    const WorldP* wp;
+    const uint32_t* wbegin;        // [nworlds + 1]
+    uint32_t nworlds, n;
+    int warm;
+    uint32_t nsteps, K, nck;
+    const unsigned long long* wk0; // the device warm cache at the start
+    const double* wi0;
+    uint32_t nw0;
+    const uint32_t* coff;          // [nworlds]
+    const uint32_t* cap;           // [nworlds]
+    uint32_t CT;
+    adj::St *S, *S0, *S1, *SB;     // [n]
+    adj::St *CKS, *SEGS;           // [nck * n], [K * n]
+    adj::Pb* PB;                   // [n]
+    adj::Con* CON;                 // [CT]
+    adj::Cb* CBS;                  // [CT]
+    double* TAPE;                  // [9 * 14 * CT]
+    unsigned long long* WK;        // [(2 + nck + K) * CT]
+    double* WI;
+    uint32_t* WN;                  // [(2 + nck + K) * nworlds]
+    double *WOB, *WIB;             // [CT]
+    const double *xbar, *vbar;     // [3n] or null
+    double *gx, *gq, *gv, *gw;     // [3n] [4n] [3n] [3n] or null
+    double *ginvm, *ginvi;         // [n] [3n]
+    double *gmu, *ge;              // [nworlds]
+    int* err;                      // [nworlds]
+};
+
+void launch_adjoint(const AdjArgs& a, cudaStream_t st);
+
 }  // namespace neb

@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "ne_adjoint.cuh"
 #include "ne_step.cuh"
 
 namespace {
@@ -1088,6 +1089,156 @@ int ne_checkpoint_destroy(NeCheckpoint* ck) {
     saved_free(ck->s);
     delete ck;
     return NE_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Device scratch of one stepBackward call, freed as a whole.
+struct Scratch {
+    std::vector<void*> ptrs;
+    ~Scratch() {
+        for (void* p : ptrs) cudaFree(p);
+    }
+    template <typename T>
+    int get(T** out, size_t count) {
+        *out = nullptr;
+        void* p = nullptr;
+        cudaError_t e = cudaMalloc(&p, (count ? count : 1) * sizeof(T));
+        if (e != cudaSuccess) return set_err(NE_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        ptrs.push_back(p);
+        *out = static_cast<T*>(p);
+        return NE_OK;
+    }
+};
+
+// One attempt at stepBackward with contact capacity cap_factor * bodies + 64
+// per world; *world_err receives the OR of the per-world error bits.
+int step_backward_once(NeWorld* w, uint32_t nsteps, uint32_t K, const NeStateGrad* fin, NeParamGrad* out,
+                       uint32_t cap_factor, int* world_err) {
+    const uint32_t n = w->n, nw = w->nworlds;
+    const uint32_t nck = (nsteps + K - 1) / K;
+    std::vector<uint32_t> coff(nw), cap(nw);
+    uint64_t CT = 0;
+    for (uint32_t k = 0; k < nw; ++k) {
+        const uint32_t nb = w->wbegin[k + 1] - w->wbegin[k];
+        cap[k] = cap_factor * nb + 64;
+        coff[k] = (uint32_t)CT;
+        CT += cap[k];
+    }
+    if (CT > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "stepBackward contact scratch exceeds 2^31 entries");
+    Scratch sc;
+    neb::AdjArgs a{};
+    a.d = w->d;
+    a.wp = w->d_wp;
+    a.nworlds = nw;
+    a.n = n;
+    a.warm = w->wparams.empty() ? (w->p.warm_start ? 1 : 0) : (w->wparams[0].warm_start ? 1 : 0);
+    a.nsteps = nsteps;
+    a.K = K;
+    a.nck = nck;
+    a.CT = (uint32_t)CT;
+    NE_CUDA_TRY(cudaMemcpy(w->h_ctl, w->d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost));
+    const uint32_t ws = w->h_ctl->wsel;
+    a.wk0 = w->d.wkey[ws];
+    a.wi0 = w->d.wimp[ws];
+    a.nw0 = a.warm ? w->h_ctl->wcount[ws] : 0;
+    int rc;
+    uint32_t *d_wbegin, *d_coff, *d_cap;
+    const size_t nslot = 2 + (size_t)nck + K;
+    if ((rc = sc.get(&d_wbegin, nw + 1)) || (rc = sc.get(&d_coff, nw)) || (rc = sc.get(&d_cap, nw)) ||
+        (rc = sc.get(&a.S, n)) || (rc = sc.get(&a.S0, n)) || (rc = sc.get(&a.S1, n)) || (rc = sc.get(&a.SB, n)) ||
+        (rc = sc.get(&a.CKS, (size_t)nck * n)) || (rc = sc.get(&a.SEGS, (size_t)K * n)) ||
+        (rc = sc.get(&a.PB, n)) || (rc = sc.get(&a.CON, CT)) || (rc = sc.get(&a.CBS, CT)) ||
+        (rc = sc.get(&a.TAPE, (size_t)9 * neb::adj::kTapeRec * CT)) || (rc = sc.get(&a.WK, nslot * CT)) ||
+        (rc = sc.get(&a.WI, nslot * CT)) || (rc = sc.get(&a.WN, nslot * nw)) || (rc = sc.get(&a.WOB, CT)) ||
+        (rc = sc.get(&a.WIB, CT)) || (rc = sc.get(&a.gx, 3 * (size_t)n)) || (rc = sc.get(&a.gq, 4 * (size_t)n)) ||
+        (rc = sc.get(&a.gv, 3 * (size_t)n)) || (rc = sc.get(&a.gw, 3 * (size_t)n)) ||
+        (rc = sc.get(&a.ginvm, n)) || (rc = sc.get(&a.ginvi, 3 * (size_t)n)) || (rc = sc.get(&a.gmu, nw)) ||
+        (rc = sc.get(&a.ge, nw)) || (rc = sc.get(&a.err, nw)))
+        return rc;
+    NE_CUDA_TRY(cudaMemcpy(d_wbegin, w->wbegin.data(), (nw + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    NE_CUDA_TRY(cudaMemcpy(d_coff, coff.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    NE_CUDA_TRY(cudaMemcpy(d_cap, cap.data(), nw * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    a.wbegin = d_wbegin;
+    a.coff = d_coff;
+    a.cap = d_cap;
+    double *xb = nullptr, *vb = nullptr;
+    if (fin && fin->x) {
+        if ((rc = sc.get(&xb, 3 * (size_t)n))) return rc;
+        NE_CUDA_TRY(cudaMemcpy(xb, fin->x, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (fin && fin->v) {
+        if ((rc = sc.get(&vb, 3 * (size_t)n))) return rc;
+        NE_CUDA_TRY(cudaMemcpy(vb, fin->v, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    a.xbar = xb;
+    a.vbar = vb;
+    neb::launch_adjoint(a, w->stream);
+    NE_CUDA_TRY(cudaGetLastError());
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    std::vector<int> err(nw);
+    NE_CUDA_TRY(cudaMemcpy(err.data(), a.err, nw * sizeof(int), cudaMemcpyDeviceToHost));
+    *world_err = 0;
+    for (int e : err) *world_err |= e;
+    if (*world_err & (neb::adj::kErrCapacity | neb::adj::kErrUnsupported)) return NE_OK;
+    if (!out) return NE_OK;
+    auto fetch = [&](double* dst, const double* src, size_t count) -> int {
+        if (!dst) return NE_OK;
+        cudaError_t e = cudaMemcpy(dst, src, count * sizeof(double), cudaMemcpyDeviceToHost);
+        return e == cudaSuccess ? NE_OK : set_err(NE_ERR_CUDA, cudaGetErrorString(e));
+    };
+    if ((rc = fetch(out->x, a.gx, 3 * (size_t)n)) || (rc = fetch(out->q, a.gq, 4 * (size_t)n)) ||
+        (rc = fetch(out->v, a.gv, 3 * (size_t)n)) || (rc = fetch(out->w, a.gw, 3 * (size_t)n)) ||
+        (rc = fetch(out->friction, a.gmu, nw)) || (rc = fetch(out->restitution, a.ge, nw)))
+        return rc;
+    std::vector<double> gim(n), gii(3 * (size_t)n);
+    NE_CUDA_TRY(cudaMemcpy(gim.data(), a.ginvm, n * sizeof(double), cudaMemcpyDeviceToHost));
+    NE_CUDA_TRY(cudaMemcpy(gii.data(), a.ginvi, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (out->inv_mass) std::memcpy(out->inv_mass, gim.data(), n * sizeof(double));
+    if (out->inv_inertia) std::memcpy(out->inv_inertia, gii.data(), 3 * (size_t)n * sizeof(double));
+    if (out->mass) {
+        // mass m: invMass = 1/m, invInertia = invInertia_0 * m_0 / m (shape fixed), so
+        // dL/dm = -(dL/dinvMass * invMass + dL/dinvInertia . invInertia) * invMass.
+        std::vector<neb::D4> pos(n), inert(n);
+        NE_CUDA_TRY(cudaMemcpy(pos.data(), w->d.pos, n * sizeof(neb::D4), cudaMemcpyDeviceToHost));
+        NE_CUDA_TRY(cudaMemcpy(inert.data(), w->d.inert, n * sizeof(neb::D4), cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < n; ++i) {
+            const double im = pos[i].w;
+            out->mass[i] = (im > 0.0) ? -(gim[i] * im + gii[3 * i] * inert[i].x + gii[3 * i + 1] * inert[i].y +
+                                          gii[3 * i + 2] * inert[i].z) * im
+                                      : 0.0;
+        }
+    }
+    return NE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ne_world_step_backward(NeWorld* w, uint32_t nsteps, uint32_t checkpoint_every, const NeStateGrad* final_grad,
+                           NeParamGrad* out) {
+    if (!w) return set_err(NE_ERR_ARG, "world is NULL");
+    if (!w->has_bodies) return set_err(NE_ERR_ARG, "world has no bodies");
+    if (nsteps == 0) return set_err(NE_ERR_ARG, "nsteps must be at least 1");
+    NE_CUDA_TRY(cudaSetDevice(w->device));
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    const uint32_t K = (checkpoint_every == 0 || checkpoint_every > nsteps) ? nsteps : checkpoint_every;
+    for (uint32_t factor = 8; factor <= 256; factor *= 2) {
+        int werr = 0;
+        int rc = step_backward_once(w, nsteps, K, final_grad, out, factor, &werr);
+        if (rc != NE_OK) return rc;
+        if (werr & neb::adj::kErrUnsupported)
+            return set_err(NE_ERR_UNSUPPORTED, "stepBackward supports open or periodic worlds of planes, boxes and "
+                                               "convex hulls (spheres with spheres and planes), <= 1024 bodies");
+        if (werr & neb::adj::kErrCapacity) continue;
+        if (werr & neb::adj::kErrNumeric)
+            return set_err(NE_ERR_NUMERIC, "an EPA or clipping budget was exceeded in the recomputed trajectory");
+        return NE_OK;
+    }
+    return set_err(NE_ERR_CAPACITY, "stepBackward contact scratch did not fit");
 }
 
 int ne_world_autotune(NeWorld* w, uint32_t steps, NeSolverShape* chosen) {

@@ -63,6 +63,7 @@ class DeviceWorld:
     def upload(self, bodies: BodyArrays):
         self._bodies = bodies
         self.n = bodies.n
+        self._wb = None
         _ffi.check(self._lib.ne_world_upload(self._h, C.byref(bodies.c)), "ne_world_upload")
 
     def upload_batch(self, params_list, bodies: BodyArrays, world_begin):
@@ -169,6 +170,31 @@ class DeviceWorld:
         s = _ffi.NeSolverShape()
         _ffi.check(self._lib.ne_world_autotune(self._h, steps, C.byref(s)), "ne_world_autotune")
         return int(s.threads), int(s.ctas_per_sm), int(s.team_max)
+
+    def step_backward(self, nsteps: int, checkpoint_every: int = 0, xbar=None, vbar=None) -> Dict[str, np.ndarray]:
+        """Gradients through the next `nsteps` steps from the current state
+        (the state is not changed), given dL/dx and dL/dv after them ([n, 3]
+        each, None = 0).  Returns x, q, v, w (initial state), mass, inv_mass,
+        inv_inertia (per body) and friction, restitution (per world)."""
+        n = self.n
+        nw = len(self._wb) - 1 if getattr(self, "_wb", None) is not None else 1
+        out = {"x": np.zeros((n, 3)), "q": np.zeros((n, 4)), "v": np.zeros((n, 3)), "w": np.zeros((n, 3)),
+               "mass": np.zeros(n), "inv_mass": np.zeros(n), "inv_inertia": np.zeros((n, 3)),
+               "friction": np.zeros(nw), "restitution": np.zeros(nw)}
+        keep = []
+
+        def dp(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            keep.append(a)
+            return a.ctypes.data_as(C.POINTER(C.c_double))
+        fin = _ffi.NeStateGrad(dp(xbar), dp(vbar))
+        pg = _ffi.NeParamGrad(*[out[k].ctypes.data_as(C.POINTER(C.c_double)) for k in
+                                ("x", "q", "v", "w", "mass", "inv_mass", "inv_inertia", "friction", "restitution")])
+        _ffi.check(self._lib.ne_world_step_backward(self._h, int(nsteps), int(checkpoint_every), C.byref(fin),
+                                                    C.byref(pg)), "ne_world_step_backward")
+        return out
 
     def checkpoint(self) -> "Checkpoint":
         """Device copy of the state and the warm cache (see restore())."""
