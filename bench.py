@@ -92,7 +92,12 @@ CONFIGS = {
                                 "(types by index mod 4), exact-overlap random sequential placement at the "
                                 "densest box that places all bodies (true-volume packing fraction ~0.19), "
                                 "v~N(0,0.5), mu=0.3, e=0.5, g=0, dt=1/60 (seed 3)"),
+    "adjoint": (None, "adjoint_512: 512 worlds of a ground plane + 64 boxes (half extent 0.5, density 1) on an "
+                      "8x8 grid, spacing 1.5, at y=0.5; v0 horizontal N(0,2^2); per-world friction U[0.2,0.8], "
+                      "restitution U[0,0.5]; g=-9.81, dt=1/60, open boundary; 120 steps, checkpoint every 10; "
+                      "loss sum |x_T - t|^2, t ~ U[-5,5]^3 (seed 6)"),
 }
+ADJ_STEPS, ADJ_K = 120, 10
 # Reference-CPU sample per config: physics steps timed on one host core.
 CPU_SAMPLE_STEPS = {"box_pile": 3, "box_pile_8": 20, "gas": 2000, "granular": 2, "batch": 2, "batch_256": 2}
 PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "solve_box_pile_512.md")
@@ -512,10 +517,128 @@ def run_ours(args):
     return 0
 
 
+def run_adjoint(args):
+    """The adjoint workload: a timed forward of the batch (fast path), a timed
+    stepBackward of the same trajectory, and a spot check of its gradients
+    against central finite differences of the FP64 reference on host cores."""
+    import torch
+    from nativeengine_b200 import DeviceWorld, scenes
+    from nativeengine_b200.shard import slice_bodies
+    from oracle import oracle as O
+    from nativeengine_b200 import _ffi
+    import ctypes as C
+
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    params, bodies, begin, targets = scenes.adjoint_batch(nworlds=512, grid=8, seed=6)
+    n = bodies.n
+    dev = DeviceWorld(params[0], None, record=False)
+    dev.upload_batch(params, bodies.copy(), begin)
+    dyn = bodies.inv_mass > 0
+    # warm-up: one forward and one backward
+    with dev.checkpoint() as ck:
+        dev.step(ADJ_STEPS)
+        xT = dev.state()["x"]
+        dev.restore(ck)
+        xbar = np.where(dyn[:, None], 2.0 * (xT - targets), 0.0)
+        dev.step_backward(ADJ_STEPS, ADJ_K, xbar=xbar)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev.step(ADJ_STEPS)
+        torch.cuda.synchronize()
+        t_fwd = time.perf_counter() - t0
+        dev.restore(ck)
+        t0 = time.perf_counter()
+        g = dev.step_backward(ADJ_STEPS, ADJ_K, xbar=xbar)
+        torch.cuda.synchronize()
+        t_bwd = time.perf_counter() - t0
+    dev.close()
+    loss = float((((xT - targets)[dyn]) ** 2).sum())
+    # Finite differences of the reference, a few parameters of a few worlds.
+    ref_cls = O.RefOracle if O.ref_available() else O.PortOracle
+
+    def wloss(p, b, tw):
+        o = ref_cls(p, b)
+        o.step(ADJ_STEPS)
+        d = (o.state()["x"] - tw)[b.inv_mass > 0]
+        return float((d * d).sum())
+
+    def pcopy(p):
+        q = _ffi.NeWorldParams()
+        C.pointer(q)[0] = p
+        return q
+    worst, nchk, nkink = 0.0, 0, 0
+    t_ref = time.perf_counter()
+    for wi in (0, 255, 511):
+        part, _ = slice_bodies(bodies, begin, wi, wi + 1)
+        tw = targets[begin[wi]:begin[wi + 1]]
+        b0 = int(begin[wi])
+        items = []
+        for li, ax in ((3, 0), (40, 2)):
+            def pv(p, b, d, li=li, ax=ax):
+                b.v[li, ax] += d
+                return p, b
+            items.append((g["v"][b0 + li, ax], pv))
+
+        def pmu(p, b, d):
+            q = pcopy(p)
+            q.friction += d
+            return q, b
+
+        def pe(p, b, d):
+            q = pcopy(p)
+            q.restitution += d
+            return q, b
+        items += [(g["friction"][wi], pmu), (g["restitution"][wi], pe)]
+        for adj, pert in items:
+            # The loss is piecewise smooth (contacts appear, support corners
+            # switch), so a fixed step can straddle a kink.  Walk h down and
+            # take the first pair of consecutive steps whose differences agree
+            # to 1e-5: the function is smooth at that scale.  The adjoint is
+            # compared with that value only; no agreeing pair = a kink within
+            # 1e-8 of the parameter (counted, not compared).
+            fds = []
+            for h in (1e-5, 1e-6, 1e-7, 1e-8):
+                lp = wloss(*pert(params[wi], part.copy(), h), tw)
+                lm = wloss(*pert(params[wi], part.copy(), -h), tw)
+                fds.append((lp - lm) / (2 * h))
+            ref_fd = None
+            for a, b in zip(fds, fds[1:]):
+                if abs(a - b) <= 1e-5 * max(abs(a), abs(b), 1e-3):
+                    ref_fd = b
+                    break
+            if ref_fd is None:
+                nkink += 1
+                continue
+            worst = max(worst, abs(adj - ref_fd) / max(abs(ref_fd), abs(adj), 1e-3))
+            nchk += 1
+    t_ref = time.perf_counter() - t_ref
+    line = {
+        "metric": "adjoint (stepBackward) throughput: body-steps/s differentiated", "value": n * ADJ_STEPS / t_bwd,
+        "unit": "body-steps/s", "n_gpus": 1, "steps": ADJ_STEPS, "warmup": 1, "ms_per_step": t_bwd / ADJ_STEPS * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": CONFIGS["adjoint"][1], "bodies": n, "worlds": 512, "checkpoint_every": ADJ_K},
+        "forward_ms": t_fwd * 1e3, "backward_ms": t_bwd * 1e3, "backward_over_forward": t_bwd / t_fwd,
+        "loss": loss,
+        "fd_check": {"max_rel_err": worst, "parameters_compared": nchk, "parameters_on_a_kink": nkink,
+                     "tolerance": 1e-4,
+                     "sample": "worlds 0, 255, 511: v0 of 2 boxes, friction, restitution; central differences of "
+                               "the FP64 reference on the host at h = 1e-5 .. 1e-8, compared at the first pair of "
+                               f"consecutive h that agree to 1e-5 ({t_ref:.1f} s)"},
+        "timing": "wall clock around synchronised calls (the backward is one kernel launch plus scratch setup)",
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "adjoint":
+        return run_adjoint(args)
     return run_ours(args)
 
 

@@ -1,5 +1,6 @@
-// ne_adjoint.cu -- stepBackward on the device: one thread per world runs the
-// per-world step program and its adjoint (ne_adjoint.cuh).
+// ne_adjoint.cu -- stepBackward on the device: one warp per world runs the
+// per-world step program and its adjoint (ne_adjoint.cuh), its lanes sharing
+// the bodies, the pairs and the islands of the world.
 //
 // Per world: (1) the state and the warm-cache entries of the world are read
 // from the device world; (2) the trajectory is stepped forward, keeping the
@@ -44,23 +45,29 @@ __device__ __forceinline__ WarmSlot warm_slot(const AdjArgs& a, uint32_t slot, u
     return s;
 }
 
-__device__ __forceinline__ void copy_warm(const WarmSlot& dst, const WarmSlot& src) {
+__device__ __forceinline__ void copy_warm(const WarmSlot& dst, const WarmSlot& src, const adj::Team& t) {
     const uint32_t n = *src.n;
-    for (uint32_t k = 0; k < n; ++k) { dst.k[k] = src.k[k]; dst.v[k] = src.v[k]; }
-    *dst.n = n;
+    for (uint32_t k = t.lane; k < n; k += t.size) { dst.k[k] = src.k[k]; dst.v[k] = src.v[k]; }
+    t.sync();
+    if (t.lane == 0) *dst.n = n;
+    t.sync();
 }
 
-__global__ void __launch_bounds__(64) k_adj_world(AdjArgs a) {
-    const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= a.nworlds) return;
+constexpr int kWarpsPerBlock = 2;
+
+// One warp per world.
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_adj_world(AdjArgs a) {
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= a.nworlds) return;   // whole warps only
+    const adj::Team t{(int)(threadIdx.x & 31), 32};
     const DevWorld& d = a.d;
     const WorldP& W = a.wp[w];
     const uint32_t b0 = a.wbegin[w], b1 = a.wbegin[w + 1], nb = b1 - b0;
     const uint32_t cap = a.cap[w];
     const int warm = a.warm;
-    a.err[w] = 0;
+    if (t.lane == 0) a.err[w] = 0;
     if (nb > kAdjMaxBodies || !adj::backward_supported(d, W, b0, b1)) {
-        a.err[w] = adj::kErrUnsupported;
+        if (t.lane == 0) a.err[w] = adj::kErrUnsupported;
         return;
     }
     adj::WScr s;
@@ -70,6 +77,7 @@ __global__ void __launch_bounds__(64) k_adj_world(AdjArgs a) {
     s.s = a.S + b0;
     s.s0 = a.S0 + b0;
     s.s1 = a.S1 + b0;
+    s.uf = a.UF + b0;
     s.con = a.CON + a.coff[w];
     s.ncon = 0;
     s.tape = nullptr;
@@ -80,22 +88,29 @@ __global__ void __launch_bounds__(64) k_adj_world(AdjArgs a) {
     adj::Pb* pb = a.PB + b0;
     double* wob = a.WOB + a.coff[w];
     double* wib = a.WIB + a.coff[w];
+    int err = 0;
 
     // Initial state and the world's entries of the warm cache (keys i<<32|j
     // with b0 <= i < b1 form one sorted run of the device cache).
-    for (uint32_t b = 0; b < nb; ++b) s.s[b] = load_state(d, b0 + b);
+    for (uint32_t b = t.lane; b < nb; b += t.size) s.s[b] = load_state(d, b0 + b);
     WarmSlot cur[2] = {warm_slot(a, 0, w), warm_slot(a, 1, w)};
     {
         const unsigned long long lo = (unsigned long long)b0 << 32, hi = (unsigned long long)b1 << 32;
         const uint32_t i0 = adj::lower_bound_key(a.wk0, a.nw0, lo), i1 = adj::lower_bound_key(a.wk0, a.nw0, hi);
         if (i1 - i0 > cap) {
-            a.err[w] = adj::kErrCapacity;
+            if (t.lane == 0) a.err[w] = adj::kErrCapacity;
             return;
         }
-        uint32_t m = 0;
-        for (uint32_t k = i0; k < i1; ++k, ++m) { cur[0].k[m] = a.wk0[k]; cur[0].v[m] = a.wi0[k]; }
-        *cur[0].n = m;
-        *cur[1].n = 0;
+        for (uint32_t k = i0 + t.lane; k < i1; k += t.size) {
+            cur[0].k[k - i0] = a.wk0[k];
+            cur[0].v[k - i0] = a.wi0[k];
+        }
+        t.sync();
+        if (t.lane == 0) {
+            *cur[0].n = i1 - i0;
+            *cur[1].n = 0;
+        }
+        t.sync();
     }
     int rd = 0;
     auto step_fwd = [&]() {
@@ -105,30 +120,36 @@ __global__ void __launch_bounds__(64) k_adj_world(AdjArgs a) {
         s.wk_out = cur[rd ^ 1].k;
         s.wi_out = cur[rd ^ 1].v;
         s.tape = nullptr;
-        adj::fwd_step(d, W, warm, s);
+        adj::fwd_step(d, W, warm, s, t);
         if (warm) {
-            *cur[rd ^ 1].n = s.nw_out;
+            t.sync();
+            if (t.lane == 0) *cur[rd ^ 1].n = s.nw_out;
+            t.sync();
             rd ^= 1;
         }
     };
     auto save = [&](St* dst, const WarmSlot& wdst) {
-        for (uint32_t b = 0; b < nb; ++b) dst[b] = s.s[b];
-        copy_warm(wdst, cur[rd]);
+        for (uint32_t b = t.lane; b < nb; b += t.size) dst[b] = s.s[b];
+        copy_warm(wdst, cur[rd], t);
     };
     auto load = [&](const St* src, const WarmSlot& wsrc) {
-        for (uint32_t b = 0; b < nb; ++b) s.s[b] = src[b];
-        copy_warm(cur[rd], wsrc);
+        for (uint32_t b = t.lane; b < nb; b += t.size) s.s[b] = src[b];
+        copy_warm(cur[rd], wsrc, t);
     };
 
     // Forward pass with checkpoints every K steps.
-    for (uint32_t t = 0; t < a.nsteps; ++t) {
-        if (t % a.K == 0) save(a.CKS + (size_t)(t / a.K) * a.n + b0, warm_slot(a, 2 + t / a.K, w));
+    for (uint32_t step = 0; step < a.nsteps; ++step) {
+        if (step % a.K == 0) save(a.CKS + (size_t)(step / a.K) * a.n + b0, warm_slot(a, 2 + step / a.K, w));
         step_fwd();
-        if (s.err & (adj::kErrCapacity | adj::kErrUnsupported)) { a.err[w] = s.err; return; }
+        if (s.err & (adj::kErrCapacity | adj::kErrUnsupported)) {
+            if (t.lane == 0) a.err[w] = s.err;
+            return;
+        }
+        err |= s.err;
     }
 
     // Adjoint of the final state.
-    for (uint32_t b = 0; b < nb; ++b) {
+    for (uint32_t b = t.lane; b < nb; b += t.size) {
         sb[b] = adj::st_zero();
         const size_t g = 3 * (size_t)(b0 + b);
         if (a.xbar) sb[b].x = mk(a.xbar[g], a.xbar[g + 1], a.xbar[g + 2]);
@@ -136,6 +157,7 @@ __global__ void __launch_bounds__(64) k_adj_world(AdjArgs a) {
         pb[b].invM = 0.0;
         pb[b].invI = mk(0.0, 0.0, 0.0);
     }
+    t.sync();
     double mub = 0.0, eb = 0.0;
     bool have_wob = false;
     const uint32_t nseg = (a.nsteps + a.K - 1) / a.K;
@@ -143,13 +165,13 @@ __global__ void __launch_bounds__(64) k_adj_world(AdjArgs a) {
         const uint32_t t0 = seg * a.K, t1 = min(a.nsteps, t0 + a.K);
         rd = 0;
         load(a.CKS + (size_t)seg * a.n + b0, warm_slot(a, 2 + seg, w));
-        for (uint32_t t = t0; t < t1; ++t) {
-            save(a.SEGS + (size_t)(t - t0) * a.n + b0, warm_slot(a, 2 + a.nck + (t - t0), w));
+        for (uint32_t step = t0; step < t1; ++step) {
+            save(a.SEGS + (size_t)(step - t0) * a.n + b0, warm_slot(a, 2 + a.nck + (step - t0), w));
             step_fwd();
         }
-        for (uint32_t t = t1; t-- > t0;) {
+        for (uint32_t step = t1; step-- > t0;) {
             rd = 0;
-            load(a.SEGS + (size_t)(t - t0) * a.n + b0, warm_slot(a, 2 + a.nck + (t - t0), w));
+            load(a.SEGS + (size_t)(step - t0) * a.n + b0, warm_slot(a, 2 + a.nck + (step - t0), w));
             s.wk_in = cur[0].k;
             s.wi_in = cur[0].v;
             s.nw_in = *cur[0].n;
@@ -157,17 +179,23 @@ __global__ void __launch_bounds__(64) k_adj_world(AdjArgs a) {
             s.wi_out = cur[1].v;
             s.tape = tape;
             s.err = 0;
-            for (uint32_t k = 0; k < s.nw_in; ++k) wib[k] = 0.0;
-            adj::bwd_step(d, W, warm, s, sb, have_wob ? wob : nullptr, wib, pb, cbs, mub, eb);
-            if (s.err & (adj::kErrCapacity | adj::kErrUnsupported)) { a.err[w] = s.err; return; }
-            a.err[w] |= s.err;
-            for (uint32_t k = 0; k < s.nw_in; ++k) wob[k] = wib[k];
+            for (uint32_t k = t.lane; k < s.nw_in; k += t.size) wib[k] = 0.0;
+            t.sync();
+            adj::bwd_step(d, W, warm, s, sb, have_wob ? wob : nullptr, wib, pb, cbs, mub, eb, t);
+            if (s.err & (adj::kErrCapacity | adj::kErrUnsupported)) {
+                if (t.lane == 0) a.err[w] = s.err;
+                return;
+            }
+            err |= s.err;
+            t.sync();
+            for (uint32_t k = t.lane; k < s.nw_in; k += t.size) wob[k] = wib[k];
+            t.sync();
             have_wob = true;
         }
     }
 
     // Outputs.
-    for (uint32_t b = 0; b < nb; ++b) {
+    for (uint32_t b = t.lane; b < nb; b += t.size) {
         const St& g = sb[b];
         const size_t i = b0 + b;
         if (a.gx) { a.gx[3 * i] = g.x.x; a.gx[3 * i + 1] = g.x.y; a.gx[3 * i + 2] = g.x.z; }
@@ -179,14 +207,17 @@ __global__ void __launch_bounds__(64) k_adj_world(AdjArgs a) {
         a.ginvi[3 * i + 1] = pb[b].invI.y;
         a.ginvi[3 * i + 2] = pb[b].invI.z;
     }
-    a.gmu[w] = mub;
-    a.ge[w] = eb;
+    if (t.lane == 0) {
+        a.gmu[w] = mub;
+        a.ge[w] = eb;
+        a.err[w] = err;
+    }
 }
 
 }  // namespace
 
 void launch_adjoint(const AdjArgs& a, cudaStream_t st) {
-    k_adj_world<<<(a.nworlds + 63) / 64, 64, 0, st>>>(a);
+    k_adj_world<<<(a.nworlds + kWarpsPerBlock - 1) / kWarpsPerBlock, 32 * kWarpsPerBlock, 0, st>>>(a);
 }
 
 }  // namespace neb

@@ -24,7 +24,7 @@
 // box-box normal comes from EPA's final face, rebuilt from its box corners.
 //
 // Everything is __host__ __device__: the device kernel (ne_adjoint.cu) runs it
-// one thread per world.
+// one warp per world (a Team of 32); the host test build runs a Team of one.
 #pragma once
 
 #include "ne_dual.cuh"
@@ -209,6 +209,7 @@ struct Con {
     double nImp0;            // warm-start impulse read from the cache
     double nImp, tImp;       // impulses during / after the solve
     int warm_idx;            // index of the cache entry it was read from, or -1
+    uint32_t own;            // team member that runs this contact's island
 };
 
 // Contact of a pair (the device narrowphase), plus EPA's final face for
@@ -390,8 +391,53 @@ struct WScr {
     double* wi_out;
     uint32_t nw_out;
     double* tape;                    // [9 * cap * 14] pre-update states of phases 0-8, or null
+    uint32_t* uf;                    // [nb] union-find parents (islands)
     int err;                         // bit 0 capacity, 1 unsupported, 2 narrowphase budget
 };
+
+// The threads that run one world: a warp on the device (lane, 32), one
+// thread on the host (0, 1).  Work with no order constraint is split over the
+// lanes; each island's solver updates run on one lane, in order.
+struct Team {
+    int lane, size;
+    NE_HD void sync() const {
+#ifdef __CUDA_ARCH__
+        __syncwarp();
+#endif
+    }
+    // Exclusive prefix of v over the lanes; *total = the sum (all lanes).
+    NE_HD uint32_t scan(uint32_t v, uint32_t& total) const {
+#ifdef __CUDA_ARCH__
+        uint32_t x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += t;
+        }
+        total = __shfl_sync(0xffffffffu, x, 31);
+        return x - v;
+#else
+        total = v;
+        return 0;
+#endif
+    }
+    NE_HD int any_or(int v) const {
+#ifdef __CUDA_ARCH__
+        for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
+#endif
+        return v;
+    }
+    NE_HD double sum(double v) const {
+#ifdef __CUDA_ARCH__
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+#endif
+        return v;
+    }
+};
+
+NE_HD uint32_t uf_root(uint32_t* p, uint32_t x) {
+    while (p[x] != x) x = p[x];
+    return x;
+}
 
 constexpr int kTapeRec = 14;
 constexpr int kErrCapacity = 1, kErrUnsupported = 2, kErrNumeric = 4;
@@ -607,6 +653,7 @@ NE_HD bool backward_supported(const DevWorld& d, const WorldP& W, uint32_t b0, u
     bool curved = false, poly = false;
     for (uint32_t i = b0; i < b1; ++i) {
         const int s = (int)d.meta[i].x;
+        if (d.meta[i].y & NE_BODY_KINEMATIC) return false;   // moving bodies shared by islands
         if (s == SH_CYLINDER || s == SH_CAPSULE || s == SH_MESH || s == SH_COMPOUND) return false;
         if (s == SH_SPHERE) curved = true;
         if (s == SH_BOX || s == SH_CONVEX) poly = true;
@@ -614,68 +661,112 @@ NE_HD bool backward_supported(const DevWorld& d, const WorldP& W, uint32_t b0, u
     return !(curved && poly);
 }
 
-// One step of world [b0, b0+nb) in place on w.s, in the reference's order.
-// With w.tape set, the post-integrate state and the input of every solver
-// update (phases 0-8) are recorded for the adjoint.
-NE_HD void fwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w) {
+// One step of world [b0, b0+nb) in place on w.s, in the reference's order,
+// run by team t (every member calls it with the same arguments; w.ncon,
+// w.nw_out and w.err come out the same on every member).  Bodies and pairs
+// are split over the members; contacts are appended in sorted pair order (a
+// prefix over the members); the solver updates of an island run on one
+// member, in the reference's order, so every body sees the reference's
+// sequence.  With w.tape set, the post-integrate state and the input of every
+// solver update (phases 0-8) are recorded for the adjoint.
+NE_HD void fwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w, const Team& t) {
     const uint32_t nb = w.nb, b0 = w.b0;
-    for (uint32_t b = 0; b < nb; ++b) {
+    for (uint32_t b = t.lane; b < nb; b += t.size) {
         w.s[b] = integrate(W, load_bc(d, b0 + b), w.s[b]);
         if (w.tape) w.s1[b] = w.s[b];
+        w.uf[b] = b;
     }
+    t.sync();
     // Pairs in sorted order, narrowphase, constraint build (k_constraint_build).
     w.ncon = 0;
+    int err = 0;
     EpaScratch S;
     for (uint32_t ia = 0; ia < nb; ++ia) {
         const Bc A = load_bc(d, b0 + ia);
-        for (uint32_t ib = ia + 1; ib < nb; ++ib) {
-            const Bc B = load_bc(d, b0 + ib);
-            if (!keep_pair(d, W.dom, b0 + ia, b0 + ib, w.s[ia], w.s[ib], A, B)) continue;
-            const BodyG ga = geom_of(d, b0 + ia, w.s[ia]), gb = geom_of(d, b0 + ib, w.s[ib]);
-            int fl = 0;
-            const PairHit h = pair_contacts(ga, gb, W.dom, S, fl);
-            if (fl & 1) w.err |= kErrNumeric;
-            if (h.n == 0) continue;
-            const double ea = A.rest < 0 ? W.restitution : A.rest, eb = B.rest < 0 ? W.restitution : B.rest;
-            const double fa = A.fric < 0 ? W.friction : A.fric, fb = B.fric < 0 ? W.friction : B.fric;
-            const double e = combine(W.rcomb, ea, eb);
-            const double mu = combine(W.fcomb, fa, fb);
-            const unsigned long long key = ((unsigned long long)(b0 + ia) << 32) | (unsigned long long)(b0 + ib);
-            const uint32_t widx = warm ? lower_bound_key(w.wk_in, w.nw_in, key) : 0u;
-            const St& sa = w.s[ia];
-            const St& sb = w.s[ib];
-            for (int k = 0; k < h.n; ++k) {
-                if (w.ncon >= w.cap) { w.err |= kErrCapacity; return; }
-                Con& c = w.con[w.ncon++];
-                c.a = ia;
-                c.b = ib;
-                c.slot = (uint32_t)k;
-                c.n = h.normal;
-                c.p = h.point[k];
-                c.ov = h.depth[k];
-                c.rA = min_image(W.dom, c.p - sa.x);
-                c.rB = min_image(W.dom, c.p - sb.x);
-                const V3 vc = (sa.v + cross(sa.w, c.rA)) - (sb.v + cross(sb.w, c.rB));
-                const double vn = dot(vc, c.n);
-                c.restBias = (vn < -0.5) ? -e * vn : 0.0;
-                c.mu = mu;
-                c.nImp0 = 0.0;
-                c.warm_idx = -1;
-                if (warm && widx + k < w.nw_in && w.wk_in[widx + k] == key) {
-                    c.nImp0 = w.wi_in[widx + k];
-                    c.warm_idx = (int)(widx + k);
+        for (uint32_t ib0 = ia + 1; ib0 < nb; ib0 += t.size) {
+            const uint32_t ib = ib0 + t.lane;
+            PairHit h;
+            h.n = 0;
+            Bc B;
+            if (ib < nb) {
+                B = load_bc(d, b0 + ib);
+                if (keep_pair(d, W.dom, b0 + ia, b0 + ib, w.s[ia], w.s[ib], A, B)) {
+                    const BodyG ga = geom_of(d, b0 + ia, w.s[ia]), gb = geom_of(d, b0 + ib, w.s[ib]);
+                    int fl = 0;
+                    h = pair_contacts(ga, gb, W.dom, S, fl);
+                    if (fl & 1) err |= kErrNumeric;
                 }
-                c.Kn = eff_mass(sa.q, A.invI, A.invM, sb.q, B.invI, B.invM, c.rA, c.rB, c.n);
-                c.nImp = c.nImp0;
-                c.tImp = 0.0;
             }
+            uint32_t total;
+            const uint32_t base = w.ncon + t.scan((uint32_t)h.n, total);
+            if (w.ncon + total > w.cap) {
+                w.err |= t.any_or(err) | kErrCapacity;
+                return;
+            }
+            if (h.n > 0) {
+                const double ea = A.rest < 0 ? W.restitution : A.rest, eb = B.rest < 0 ? W.restitution : B.rest;
+                const double fa = A.fric < 0 ? W.friction : A.fric, fb = B.fric < 0 ? W.friction : B.fric;
+                const double e = combine(W.rcomb, ea, eb);
+                const double mu = combine(W.fcomb, fa, fb);
+                const unsigned long long key = ((unsigned long long)(b0 + ia) << 32) | (unsigned long long)(b0 + ib);
+                const uint32_t widx = warm ? lower_bound_key(w.wk_in, w.nw_in, key) : 0u;
+                const St& sa = w.s[ia];
+                const St& sb = w.s[ib];
+                for (int k = 0; k < h.n; ++k) {
+                    Con& c = w.con[base + k];
+                    c.a = ia;
+                    c.b = ib;
+                    c.slot = (uint32_t)k;
+                    c.n = h.normal;
+                    c.p = h.point[k];
+                    c.ov = h.depth[k];
+                    c.rA = min_image(W.dom, c.p - sa.x);
+                    c.rB = min_image(W.dom, c.p - sb.x);
+                    const V3 vc = (sa.v + cross(sa.w, c.rA)) - (sb.v + cross(sb.w, c.rB));
+                    const double vn = dot(vc, c.n);
+                    c.restBias = (vn < -0.5) ? -e * vn : 0.0;
+                    c.mu = mu;
+                    c.nImp0 = 0.0;
+                    c.warm_idx = -1;
+                    if (warm && widx + k < w.nw_in && w.wk_in[widx + k] == key) {
+                        c.nImp0 = w.wi_in[widx + k];
+                        c.warm_idx = (int)(widx + k);
+                    }
+                    c.Kn = eff_mass(sa.q, A.invI, A.invM, sb.q, B.invI, B.invM, c.rA, c.rB, c.n);
+                    c.nImp = c.nImp0;
+                    c.tImp = 0.0;
+                }
+            }
+            w.ncon += total;
         }
     }
-    // Warm start, 8 sweeps (phases 0-8), on the post-integrate orientations.
+    w.err |= t.any_or(err);
+    t.sync();
+    // Islands over the mutable bodies (union-find on member 0); each island
+    // goes to the member root % size.
+    const uint32_t nc = w.ncon;
+    if (t.lane == 0) {
+        for (uint32_t ci = 0; ci < nc; ++ci) {
+            const Con& c = w.con[ci];
+            if (!mutable_(load_bc(d, b0 + c.a)) || !mutable_(load_bc(d, b0 + c.b))) continue;
+            const uint32_t ra = uf_root(w.uf, c.a), rb = uf_root(w.uf, c.b);
+            if (ra != rb) w.uf[ra > rb ? ra : rb] = ra < rb ? ra : rb;
+        }
+    }
+    t.sync();
+    for (uint32_t ci = t.lane; ci < nc; ci += t.size) {
+        Con& c = w.con[ci];
+        const uint32_t body = mutable_(load_bc(d, b0 + c.a)) ? c.a : c.b;
+        c.own = uf_root(w.uf, body) % (uint32_t)t.size;
+    }
+    t.sync();
+    // Warm start, 8 sweeps (phases 0-8), on the post-integrate orientations;
+    // then position correction (correct_item) and the warm cache.
     for (int ph = 0; ph <= 8; ++ph) {
         if (ph == 0 && !warm) continue;
-        for (uint32_t ci = 0; ci < w.ncon; ++ci) {
+        for (uint32_t ci = 0; ci < nc; ++ci) {
             Con& c = w.con[ci];
+            if (c.own != (uint32_t)t.lane) continue;
             const Bc A = load_bc(d, b0 + c.a), B = load_bc(d, b0 + c.b);
             St& sa = w.s[c.a];
             St& sb = w.s[c.b];
@@ -692,10 +783,9 @@ NE_HD void fwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w) {
             if (mutable_(B)) { sb.v = vB; sb.w = wB; }
         }
     }
-    // Position correction (correct_item) and the warm cache.
-    w.nw_out = 0;
-    for (uint32_t ci = 0; ci < w.ncon; ++ci) {
+    for (uint32_t ci = 0; ci < nc; ++ci) {
         const Con& c = w.con[ci];
+        if (c.own != (uint32_t)t.lane) continue;
         const Bc A = load_bc(d, b0 + c.a), B = load_bc(d, b0 + c.b);
         const double invSum = A.invM + B.invM;
         if (!(invSum <= 0.0 || c.ov <= 0.0)) {
@@ -706,12 +796,13 @@ NE_HD void fwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w) {
         if (warm) {
             w.wk_out[ci] = ((unsigned long long)(b0 + c.a) << 32) | (unsigned long long)(b0 + c.b);
             w.wi_out[ci] = c.nImp;
-            w.nw_out = ci + 1;
         }
     }
+    w.nw_out = warm ? nc : 0;
+    t.sync();
     // wrapPositions / applyWalls (world.cpp:698-702, 635-657; k_boundary).
     // The adjoint differentiates open and periodic worlds only.
-    for (uint32_t b = 0; b < nb; ++b) {
+    for (uint32_t b = t.lane; b < nb; b += t.size) {
         if (!(load_bc(d, b0 + b).invM > 0.0)) continue;
         St& s = w.s[b];
         if (W.dom.periodic) {
@@ -740,6 +831,7 @@ NE_HD void fwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w) {
         s.x = mk(px[0], px[1], px[2]);
         s.v = mk(pv[0], pv[1], pv[2]);
     }
+    t.sync();
 }
 
 // ---- contact geometry in dual numbers -----------------------------------------
@@ -876,26 +968,45 @@ NE_HD void acc_dual(const Vec3<Dual>& v, const V3& vb, double* g) {
 // (inverse mass and inertia) are accumulated, and so are mub / eb (world
 // friction / restitution, through the bodies that inherit them).  cbs[cap] is
 // scratch.  The recomputed forward leaves w.s at the state after the step.
+// Run by team t like fwd_step: the reverse of an island's updates runs on the
+// member that ran them; adjoints of immovable bodies (which carry no
+// gradient: zero inverse mass and inertia) go to a member-local sink, so no
+// two members write the same memory.
 NE_HD void bwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w, St* sb, const double* wob, double* wib,
-                    Pb* pb, Cb* cbs, double& mub, double& eb) {
+                    Pb* pb, Cb* cbs, double& mub, double& eb, const Team& t) {
     const uint32_t nb = w.nb, b0 = w.b0;
-    for (uint32_t b = 0; b < nb; ++b) w.s0[b] = w.s[b];
-    fwd_step(d, W, warm, w);
+    for (uint32_t b = t.lane; b < nb; b += t.size) w.s0[b] = w.s[b];
+    t.sync();
+    fwd_step(d, W, warm, w, t);
     if (w.err & (kErrCapacity | kErrUnsupported)) return;
     const uint32_t nc = w.ncon;
-    for (uint32_t ci = 0; ci < nc; ++ci) {
+    for (uint32_t ci = t.lane; ci < nc; ci += t.size) {
         cbs[ci] = cb_zero();
         if (warm && wob) cbs[ci].ixb = wob[ci];
     }
+    t.sync();
+    const uint32_t me = (uint32_t)t.lane;
+    St sink_s;
+    Pb sink_p;
+    double mub_l = 0.0, eb_l = 0.0;
+    // Body adjoint / parameter accumulators of a contact's body (the sink for
+    // an immovable one).
+#define NE_ADJ_BODY(Bvar, li, S_, P_)                         \
+    St* S_ = &sink_s;                                       \
+    Pb* P_ = &sink_p;                                       \
+    if (mutable_(Bvar)) { S_ = &sb[li]; P_ = &pb[li]; }      \
+    else { sink_s = st_zero(); sink_p.invM = 0.0; sink_p.invI = mk(0.0, 0.0, 0.0); }
     // Position correction (x passes through; the correction's operands get adjoints).
     for (uint32_t ci = nc; ci-- > 0;) {
         const Con& c = w.con[ci];
+        if (c.own != me) continue;
         const Bc A = load_bc(d, b0 + c.a), B = load_bc(d, b0 + c.b);
         const double invSum = A.invM + B.invM;
         if (invSum <= 0.0 || c.ov <= 0.0) continue;
         const double k = W.beta * c.ov / invSum;
         const V3 corr = c.n * k;
         V3 corrb = mk(0.0, 0.0, 0.0);
+        double invSumb;
         if (mutable_(A)) {
             add(corrb, sb[c.a].x * A.invM);
             pb[c.a].invM += dot(sb[c.a].x, corr);
@@ -907,29 +1018,35 @@ NE_HD void bwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w, St* s
         add(cbs[ci].n, corrb * k);
         const double kb = dot(corrb, c.n);
         cbs[ci].ov += kb * W.beta / invSum;
-        const double invSumb = -kb * W.beta * c.ov / (invSum * invSum);
-        pb[c.a].invM += invSumb;
-        pb[c.b].invM += invSumb;
+        invSumb = -kb * W.beta * c.ov / (invSum * invSum);
+        if (mutable_(A)) pb[c.a].invM += invSumb;
+        if (mutable_(B)) pb[c.b].invM += invSumb;
     }
     // Sweeps 8..1, then the warm start, in reverse order.
     for (int ph = 8; ph >= 0; --ph) {
         if (ph == 0 && !warm) break;
         for (uint32_t ci = nc; ci-- > 0;) {
             const Con& c = w.con[ci];
+            if (c.own != me) continue;
             Cb& cb = cbs[ci];
             const Bc A = load_bc(d, b0 + c.a), B = load_bc(d, b0 + c.b);
             const Sk kA = sk_of(A, w.s1[c.a]), kB = sk_of(B, w.s1[c.b]);
-            St& ba = sb[c.a];
-            St& bb = sb[c.b];
+            NE_ADJ_BODY(A, c.a, ba, pa)
+            St sink_b;
+            Pb sink_pb;
+            St* bb = &sink_b;
+            Pb* pbb = &sink_pb;
+            if (mutable_(B)) { bb = &sb[c.b]; pbb = &pb[c.b]; }
+            else { sink_b = st_zero(); sink_pb.invM = 0.0; sink_pb.invI = mk(0.0, 0.0, 0.0); }
             if (ph > 0) {
-                sweep_vjp(c, kA, kB, w.tape + ((size_t)ph * w.cap + ci) * kTapeRec, ba.v, ba.w, bb.v, bb.w, cb.ixb,
-                          cb.iyb, cb, ba.q, pb[c.a], bb.q, pb[c.b]);
+                sweep_vjp(c, kA, kB, w.tape + ((size_t)ph * w.cap + ci) * kTapeRec, ba->v, ba->w, bb->v, bb->w,
+                          cb.ixb, cb.iyb, cb, ba->q, *pa, bb->q, *pbb);
                 continue;
             }
             if (c.nImp0 == 0.0) continue;
             const V3 J = c.n * c.nImp0;
             V3 Jb = mk(0.0, 0.0, 0.0);
-            apply_pair_vjp(kA, kB, c.rA, c.rB, J, ba.v, ba.w, bb.v, bb.w, Jb, ba.q, pb[c.a], bb.q, pb[c.b], cb.rA,
+            apply_pair_vjp(kA, kB, c.rA, c.rB, J, ba->v, ba->w, bb->v, bb->w, Jb, ba->q, *pa, bb->q, *pbb, cb.rA,
                            cb.rB);
             add(cb.n, Jb * c.nImp0);
             cb.ixb += dot(Jb, c.n);
@@ -938,12 +1055,18 @@ NE_HD void bwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w, St* s
     // Constraint build: rA, rB, restitution bias, friction, Kn, warm impulse.
     for (uint32_t ci = 0; ci < nc; ++ci) {
         const Con& c = w.con[ci];
+        if (c.own != me) continue;
         Cb& cb = cbs[ci];
         const Bc A = load_bc(d, b0 + c.a), B = load_bc(d, b0 + c.b);
         const St& sa = w.s1[c.a];
         const St& sbb = w.s1[c.b];
-        St& ba = sb[c.a];
-        St& bb = sb[c.b];
+        NE_ADJ_BODY(A, c.a, ba, pa)
+        St sink_b;
+        Pb sink_pb;
+        St* bb = &sink_b;
+        Pb* pbb = &sink_pb;
+        if (mutable_(B)) { bb = &sb[c.b]; pbb = &pb[c.b]; }
+        else { sink_b = st_zero(); sink_pb.invM = 0.0; sink_pb.invI = mk(0.0, 0.0, 0.0); }
         if (warm && c.warm_idx >= 0 && wib) wib[c.warm_idx] += cb.ixb;
         // restitution bias from the pre-solve velocities
         const V3 vc = (sa.v + cross(sa.w, c.rA)) - (sbb.v + cross(sbb.w, c.rB));
@@ -954,63 +1077,73 @@ NE_HD void bwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w, St* s
             const double e_b = -vn * cb.restBias;
             double gx, gy;
             combine_grad(W.rcomb, ea, ebv, gx, gy);
-            if (A.rest < 0) eb += e_b * gx;
-            if (B.rest < 0) eb += e_b * gy;
+            if (A.rest < 0) eb_l += e_b * gx;
+            if (B.rest < 0) eb_l += e_b * gy;
             const double vnb = -e * cb.restBias;
             const V3 vcb = c.n * vnb;
             add(cb.n, vc * vnb);
-            add(ba.v, vcb);
-            cross_vjp(sa.w, c.rA, vcb, ba.w, cb.rA);
-            bb.v = bb.v - vcb;
-            cross_vjp(sbb.w, c.rB, -vcb, bb.w, cb.rB);
+            add(ba->v, vcb);
+            cross_vjp(sa.w, c.rA, vcb, ba->w, cb.rA);
+            bb->v = bb->v - vcb;
+            cross_vjp(sbb.w, c.rB, -vcb, bb->w, cb.rB);
         }
         {
             const double fa = A.fric < 0 ? W.friction : A.fric, fb = B.fric < 0 ? W.friction : B.fric;
             double gx, gy;
             combine_grad(W.fcomb, fa, fb, gx, gy);
-            if (A.fric < 0) mub += cb.mu * gx;
-            if (B.fric < 0) mub += cb.mu * gy;
+            if (A.fric < 0) mub_l += cb.mu * gx;
+            if (B.fric < 0) mub_l += cb.mu * gy;
         }
         const Sk kA = sk_of(A, sa), kB = sk_of(B, sbb);
-        effmass_vjp(kA, kB, c.rA, c.rB, c.n, cb.Kn, ba.q, pb[c.a], bb.q, pb[c.b], cb.rA, cb.rB, cb.n);
+        effmass_vjp(kA, kB, c.rA, c.rB, c.n, cb.Kn, ba->q, *pa, bb->q, *pbb, cb.rA, cb.rB, cb.n);
         add(cb.p, cb.rA + cb.rB);
-        ba.x = ba.x - cb.rA;
-        bb.x = bb.x - cb.rB;
+        ba->x = ba->x - cb.rA;
+        bb->x = bb->x - cb.rB;
     }
     // Contact geometry: normal, points and depths as functions of both poses.
     {
         EpaScratch S;
         uint32_t ci = 0;
+        int gerr = 0;
         while (ci < nc) {
             uint32_t cj = ci;
             while (cj < nc && w.con[cj].a == w.con[ci].a && w.con[cj].b == w.con[ci].b) ++cj;
             const Con& c = w.con[ci];
-            const BodyG ga = geom_of(d, b0 + c.a, w.s1[c.a]), gbd = geom_of(d, b0 + c.b, w.s1[c.b]);
-            PairDual pd;
-            if (!pair_contacts_dual(ga, gbd, W.dom, S, pd) || pd.n != (int)(cj - ci)) {
-                w.err |= kErrUnsupported;
-                return;
+            if (c.own == me) {
+                const BodyG ga = geom_of(d, b0 + c.a, w.s1[c.a]), gbd = geom_of(d, b0 + c.b, w.s1[c.b]);
+                PairDual pd;
+                if (!pair_contacts_dual(ga, gbd, W.dom, S, pd) || pd.n != (int)(cj - ci)) {
+                    gerr = kErrUnsupported;
+                } else {
+                    double g[kDualDirs];
+                    for (int k = 0; k < kDualDirs; ++k) g[k] = 0.0;
+                    for (uint32_t k = ci; k < cj; ++k) {
+                        const Cb& cb = cbs[k];
+                        const int s = (int)(k - ci);
+                        acc_dual(pd.normal, cb.n, g);
+                        acc_dual(pd.point[s], cb.p, g);
+                        for (int q = 0; q < kDualDirs; ++q) g[q] += cb.ov * pd.depth[s].d[q];
+                    }
+                    const Bc A = load_bc(d, b0 + c.a), B = load_bc(d, b0 + c.b);
+                    if (mutable_(A)) {
+                        add(sb[c.a].x, mk(g[0], g[1], g[2]));
+                        addq(sb[c.a].q, mkq(g[3], g[4], g[5], g[6]));
+                    }
+                    if (mutable_(B)) {
+                        add(sb[c.b].x, mk(g[7], g[8], g[9]));
+                        addq(sb[c.b].q, mkq(g[10], g[11], g[12], g[13]));
+                    }
+                }
             }
-            double g[kDualDirs];
-            for (int k = 0; k < kDualDirs; ++k) g[k] = 0.0;
-            for (uint32_t k = ci; k < cj; ++k) {
-                const Cb& cb = cbs[k];
-                const int s = (int)(k - ci);
-                acc_dual(pd.normal, cb.n, g);
-                acc_dual(pd.point[s], cb.p, g);
-                for (int t = 0; t < kDualDirs; ++t) g[t] += cb.ov * pd.depth[s].d[t];
-            }
-            St& ba = sb[c.a];
-            St& bb = sb[c.b];
-            add(ba.x, mk(g[0], g[1], g[2]));
-            addq(ba.q, mkq(g[3], g[4], g[5], g[6]));
-            add(bb.x, mk(g[7], g[8], g[9]));
-            addq(bb.q, mkq(g[10], g[11], g[12], g[13]));
             ci = cj;
         }
+        w.err |= t.any_or(gerr);
+        if (w.err & kErrUnsupported) return;
     }
+#undef NE_ADJ_BODY
+    t.sync();
     // Integration (World::integrate) per body.
-    for (uint32_t b = 0; b < nb; ++b) {
+    for (uint32_t b = t.lane; b < nb; b += t.size) {
         const Bc B = load_bc(d, b0 + b);
         const St& s0 = w.s0[b];
         St& g = sb[b];
@@ -1047,6 +1180,9 @@ NE_HD void bwd_step(const DevWorld& d, const WorldP& W, int warm, WScr& w, St* s
         }
         sb[b] = o;
     }
+    t.sync();
+    mub += t.sum(mub_l);
+    eb += t.sum(eb_l);
 }
 
 }  // namespace adj
@@ -1075,6 +1211,7 @@ struct AdjArgs {
     const uint32_t* cap;           // [nworlds]
     uint32_t CT;
     adj::St *S, *S0, *S1, *SB;     // [n]
+    uint32_t* UF;                  // [n] union-find scratch
     adj::St *CKS, *SEGS;           // [nck * n], [K * n]
     adj::Pb* PB;                   // [n]
     adj::Con* CON;                 // [CT]

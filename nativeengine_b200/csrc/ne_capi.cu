@@ -1149,6 +1149,7 @@ int step_backward_once(NeWorld* w, uint32_t nsteps, uint32_t K, const NeStateGra
     const size_t nslot = 2 + (size_t)nck + K;
     if ((rc = sc.get(&d_wbegin, nw + 1)) || (rc = sc.get(&d_coff, nw)) || (rc = sc.get(&d_cap, nw)) ||
         (rc = sc.get(&a.S, n)) || (rc = sc.get(&a.S0, n)) || (rc = sc.get(&a.S1, n)) || (rc = sc.get(&a.SB, n)) ||
+        (rc = sc.get(&a.UF, n)) ||
         (rc = sc.get(&a.CKS, (size_t)nck * n)) || (rc = sc.get(&a.SEGS, (size_t)K * n)) ||
         (rc = sc.get(&a.PB, n)) || (rc = sc.get(&a.CON, CT)) || (rc = sc.get(&a.CBS, CT)) ||
         (rc = sc.get(&a.TAPE, (size_t)9 * neb::adj::kTapeRec * CT)) || (rc = sc.get(&a.WK, nslot * CT)) ||

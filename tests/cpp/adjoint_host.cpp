@@ -88,6 +88,7 @@ void build(HostWorld& h, const NeWorldParams* p, const NeBodyArrays* b) {
 
 struct Run {
     std::vector<adj::St> s, s0, s1;
+    std::vector<uint32_t> uf;
     std::vector<adj::Con> con;
     std::vector<double> tape;
     std::vector<unsigned long long> wk[2];
@@ -98,7 +99,7 @@ struct Run {
 
     void init(const HostWorld& h, uint32_t capacity) {
         cap = capacity;
-        s.resize(h.n); s0.resize(h.n); s1.resize(h.n);
+        s.resize(h.n); s0.resize(h.n); s1.resize(h.n); uf.resize(h.n);
         for (uint32_t i = 0; i < h.n; ++i) {
             adj::St& t = s[i];
             t.x = mk(h.pos[i].x, h.pos[i].y, h.pos[i].z);
@@ -113,6 +114,7 @@ struct Run {
         for (int k = 0; k < 2; ++k) { wk[k].assign(cap, 0); wi[k].assign(cap, 0.0); }
         w.b0 = 0; w.nb = h.n; w.cap = cap;
         w.s = s.data(); w.s0 = s0.data(); w.s1 = s1.data(); w.con = con.data(); w.tape = tape.data();
+        w.uf = uf.data();
     }
 
     // One forward step reading warm cache `rd`, writing the other.
@@ -121,7 +123,7 @@ struct Run {
         w.wk_out = wk[rd ^ 1].data(); w.wi_out = wi[rd ^ 1].data();
         w.tape = with_tape ? tape.data() : nullptr;
         w.err = 0;
-        adj::fwd_step(h.d, h.W, h.warm, w);
+        adj::fwd_step(h.d, h.W, h.warm, w, adj::Team{0, 1});
         nw[rd ^ 1] = w.nw_out;
         return w.err;
     }
@@ -202,7 +204,7 @@ int adjh_grad(const NeWorldParams* p, const NeBodyArrays* b, int nsteps, uint32_
         r.w.err = 0;
         wib.assign(cap, 0.0);
         adj::bwd_step(h.d, h.W, h.warm, r.w, sb.data(), wob.empty() ? nullptr : wob.data(), wib.data(), pb.data(),
-                      cbs.data(), mub, eb);
+                      cbs.data(), mub, eb, adj::Team{0, 1});
         if (r.w.err & (adj::kErrCapacity | adj::kErrUnsupported)) return r.w.err;
         wob = wib;   // the warm impulses read by step k were stored by step k - 1
     }
