@@ -428,15 +428,23 @@ def run_ours(args):
         ms = [a.elapsed_time(b) for a, b in zip(ev0, ev1)]
         return ms, launches
 
-    dev.profile(True)
     sampler = ClockSampler(local)
     sampler.start()
     ms_dev, launches = timed_run(host_io=False)
     clocks = sampler.stop()
-    stages = dev.stage_times()
     stats = dev.stats()
-    dev.profile(False)
     ms_e2e, _ = timed_run(host_io=True)
+    # Stage breakdown: a separate run of the same steps with CUDA events
+    # between the stages (which steps kernel by kernel, outside the graph).
+    if begin is None:
+        dev.upload(bodies.copy())
+    else:
+        dev.upload_batch(params, bodies.copy(), begin)
+    dev.reset_warm_cache()
+    dev.profile(True)
+    dev.step(args.steps)
+    stages = dev.stage_times()
+    dev.profile(False)
     fp32_err = fp32_one_step_error(dev) if args.precision == "f32" else None
 
     t_dev = sum(ms_dev) / 1e3
@@ -483,7 +491,10 @@ def run_ours(args):
                        "parallelism": (f"dp{world}: worlds sharded by body count, no data-path collective"
                                        if sharded else ("replicas" if world > 1 else
                                                         ("batch of worlds" if begin is not None else "single world"))),
-                       "l2": "256 MiB buffer rewritten between timed steps (outside the events)"},
+                       "l2": "256 MiB buffer rewritten between timed steps (outside the events)",
+                       "step_launch": "CUDA graph of the whole step, replayed once per step; one read of the "
+                                      "device control block per step",
+                       "graph_steps": stats["graph_steps"]},
             "roofline": {"bound": "hbm", "kernel": "solve (k_island_solve + k_island_solve_local)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "traffic": profile_traffic(C_last),

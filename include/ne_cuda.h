@@ -164,6 +164,8 @@ typedef struct NeStepStats {
     uint64_t steps;          /* steps taken since upload                      */
     uint64_t retries;        /* steps re-run after growing a device buffer    */
     uint64_t candidates;     /* pairs the internal grid handed to the cull    */
+    uint64_t graph_steps;    /* steps run by replaying the captured step graph */
+    uint64_t graph_captures; /* times the step graph was (re)captured         */
 } NeStepStats;
 
 typedef struct NeWorld NeWorld;
@@ -312,8 +314,20 @@ int ne_world_step_backward(NeWorld* world, uint32_t nsteps, uint32_t checkpoint_
 
 /* The CUDA stream the world launches on (as a void*; cast to cudaStream_t). */
 int ne_world_stream(const NeWorld* world, void** stream);
-/* Number of kernel launches made by the last ne_world_step call. */
+/* Number of kernel launches made by the last ne_world_step call (kernels
+ * inside replayed graphs included). */
 int ne_world_launch_count(const NeWorld* world, uint64_t* launches);
+
+/* CUDA-graph stepping (on by default; no counterpart in the reference).  The
+ * kernels of one step are captured once into a CUDA graph and replayed in
+ * batches of up to 64 steps, with one read of the control block per batch
+ * instead of one per step.  A step that overflows a device buffer halts the
+ * rest of its batch on the device; the host restores that step's pre-step
+ * state, grows the buffer and takes the step again outside the graph, so
+ * results are the same bit for bit with the graph on or off.  Changing
+ * capacities, precision, solver shape or parameters re-captures the graph.
+ * Steps with stage timing or pair recording enabled run outside the graph. */
+int ne_world_set_graph(NeWorld* world, int enable);
 
 /* Per-stage device timing (CUDA events on the world's stream).  Stages:
  * 0 integrate, 1 broadphase, 2 pair filter + cull, 3 narrowphase,

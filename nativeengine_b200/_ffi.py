@@ -109,6 +109,7 @@ class NeStepStats(C.Structure):
         ("pairs", C.c_uint64), ("survivors", C.c_uint64), ("contacts", C.c_uint64),
         ("islands", C.c_uint64), ("max_island", C.c_uint64), ("epa_cap_hits", C.c_uint64),
         ("steps", C.c_uint64), ("retries", C.c_uint64), ("candidates", C.c_uint64),
+        ("graph_steps", C.c_uint64), ("graph_captures", C.c_uint64),
     ]
 
 
@@ -131,6 +132,7 @@ EXPORTS = {
     "ne_world_islands": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32]),
     "ne_world_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "ne_world_launch_count": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64)]),
+    "ne_world_set_graph": (C.c_int, [C.c_void_p, C.c_int]),
     "ne_world_set_record": (C.c_int, [C.c_void_p, C.c_uint32]),
     "ne_world_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
     "ne_world_set_solver_shape": (C.c_int, [C.c_void_p, C.POINTER(NeSolverShape)]),

@@ -99,6 +99,12 @@ struct NeWorld {
     NeStepStats stats{};
     uint64_t launches = 0;
     bool has_bodies = false;
+    // CUDA graph of one step, replayed for batches of steps; valid while
+    // make_args() returns the arguments it was captured with.
+    bool graph_on = true;
+    cudaGraphExec_t gexec = nullptr;
+    neb::StepArgs gargs{};
+    uint64_t g_launches = 0;              // kernels in the captured step
     // stage timing
     bool profile = false;
     cudaEvent_t ev[NE_NUM_STAGES + 1] = {};
@@ -246,6 +252,7 @@ int alloc_cons(NeWorld* w, uint64_t cap) {
 
 neb::StepArgs make_args(const NeWorld* w) {
     neb::StepArgs a;
+    std::memset(&a, 0, sizeof a);   // padding too: captured arguments are compared bytewise
     a.d = w->d;
     a.n = w->n;
     a.nworlds = w->nworlds;
@@ -472,6 +479,7 @@ int ne_world_destroy(NeWorld* w) {
     if (w->pinned) cudaFreeHost(w->pinned);
     for (int k = 0; k <= NE_NUM_STAGES; ++k)
         if (w->ev[k]) cudaEventDestroy(w->ev[k]);
+    if (w->gexec) cudaGraphExecDestroy(w->gexec);
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
     return NE_OK;
@@ -683,6 +691,162 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
     return NE_OK;
 }
 
+// Copies the pre-step snapshot k_integrate took back into the state: undoes
+// the integration of a step that aborted.
+int restore_pre_step(NeWorld* w) {
+    const size_t bytes = (size_t)w->n * sizeof(neb::D4);
+    neb::DevWorld& d = w->d;
+    NE_CUDA_TRY(cudaMemcpyAsync(d.pos, d.s_pos, bytes, cudaMemcpyDeviceToDevice, w->stream));
+    NE_CUDA_TRY(cudaMemcpyAsync(d.quat, d.s_quat, bytes, cudaMemcpyDeviceToDevice, w->stream));
+    NE_CUDA_TRY(cudaMemcpyAsync(d.vel, d.s_vel, bytes, cudaMemcpyDeviceToDevice, w->stream));
+    NE_CUDA_TRY(cudaMemcpyAsync(d.omg, d.s_omg, bytes, cudaMemcpyDeviceToDevice, w->stream));
+    NE_CUDA_TRY(cudaMemcpyAsync(d.frc, d.s_frc, bytes, cudaMemcpyDeviceToDevice, w->stream));
+    NE_CUDA_TRY(cudaMemcpyAsync(d.trq, d.s_trq, bytes, cudaMemcpyDeviceToDevice, w->stream));
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    return NE_OK;
+}
+
+// Grows what an aborted step (its counts in c) overflowed.
+int grow_for(NeWorld* w, const neb::Ctl& c) {
+    int rc = NE_OK;
+    bool grew = false;
+    if ((int)c.need_bits > w->key_bits) {
+        w->key_bits = (((int)c.need_bits + 7) / 8) * 8;
+        grew = true;
+    }
+    if (c.P_ref > w->Rcap && (w->record & NE_RECORD_PAIRS)) {
+        if (c.P_ref > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 recorded pairs");
+        if ((rc = alloc_rec(w, grow_to(c.P_ref)))) return rc;
+        grew = true;
+    } else if (c.S > w->Scap) {
+        if (c.S > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 surviving pairs");
+        if ((rc = alloc_surv(w, grow_to(c.S)))) return rc;
+        grew = true;
+    } else if (c.C > w->Ccap) {
+        if (c.C > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 contacts");
+        if ((rc = alloc_cons(w, grow_to(c.C)))) return rc;
+        grew = true;
+    }
+    if (!grew) return set_err(NE_ERR_CAPACITY, "step aborted without a growable cause");
+    if ((rc = alloc_scratch(w))) return rc;
+    ++w->stats.retries;
+    return NE_OK;
+}
+
+// Counters of the last completed step (c holds its ctl block).
+void take_step_counts(NeWorld* w, const neb::Ctl& c) {
+    w->stats.pairs = (w->record & NE_RECORD_PAIRS) ? c.P_ref : c.P;
+    w->stats.candidates = c.P;
+    w->stats.survivors = c.S;
+    w->stats.contacts = c.C;
+    w->stats.islands = c.islands;
+    w->stats.max_island = c.max_island;
+}
+
+// One step, launched kernel by kernel, re-run after growth until it fits.
+int step_eager(NeWorld* w, int* status) {
+    for (int attempt = 0;; ++attempt) {
+        if (attempt > 16) return set_err(NE_ERR_CAPACITY, "step did not fit after repeated growth");
+        neb::StepArgs a = make_args(w);
+        neb::launch_step(a, w->stream, &w->launches, w->profile ? w->ev : nullptr);
+        NE_CUDA_TRY(cudaGetLastError());
+        NE_CUDA_TRY(cudaMemcpyAsync(w->h_ctl, w->d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost, w->stream));
+        NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+        const neb::Ctl& c = *w->h_ctl;
+        if (!c.abort) break;
+        int rc;
+        if ((rc = restore_pre_step(w)) || (rc = grow_for(w, *w->h_ctl))) return rc;
+    }
+    const neb::Ctl& c = *w->h_ctl;
+    if (w->profile) {
+        for (int k = 0; k < NE_NUM_STAGES; ++k) {
+            float ms = 0.f;
+            NE_CUDA_TRY(cudaEventElapsedTime(&ms, w->ev[k], w->ev[k + 1]));
+            w->stage_ms[k] += ms;
+        }
+        ++w->stage_steps;
+    }
+    // Shrink the cell-key sort to the bits this step needed.
+    if (w->any_grid) {
+        int kb = (((int)c.need_bits + 7) / 8) * 8;
+        if (kb >= 8) w->key_bits = kb;
+    }
+    take_step_counts(w, c);
+    w->stats.epa_cap_hits += c.epa_cap_hits;
+    w->stats.steps += 1;
+    if (c.solve_timeout) return set_err(NE_ERR_TIMEOUT, "a dataflow-solver dependency wait ran out");
+    if (c.flags & 1u) *status = set_err(NE_ERR_NUMERIC, "an EPA or clipping budget was exceeded");
+    return NE_OK;
+}
+
+// Steps per replayed batch: the host reads the control block once per batch.
+constexpr uint32_t kGraphBatch = 64;
+
+// Stage timing records events between kernels and recording builds a second
+// pair list into a host-sized buffer: both step kernel by kernel.
+bool graph_usable(const NeWorld* w) { return w->graph_on && !w->profile && !(w->record & NE_RECORD_PAIRS); }
+
+// Up to min(want, kGraphBatch) steps by replaying the captured step (captured
+// again first if the arguments changed).  *done = steps completed; *halted =
+// the next step overflowed a buffer, its pre-step state has been restored
+// and the buffer grown.
+int step_graph_batch(NeWorld* w, uint32_t want, uint32_t* done, bool* halted, int* status) {
+    neb::StepArgs a = make_args(w);
+    a.sticky = 1;
+    if (!w->gexec || std::memcmp(&a, &w->gargs, sizeof a) != 0) {
+        if (w->gexec) {
+            NE_CUDA_TRY(cudaGraphExecDestroy(w->gexec));
+            w->gexec = nullptr;
+        }
+        uint64_t L = 0;
+        cudaGraph_t g = nullptr;
+        NE_CUDA_TRY(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
+        neb::launch_step(a, w->stream, &L, nullptr);
+        const cudaError_t le = cudaGetLastError();
+        const cudaError_t ce = cudaStreamEndCapture(w->stream, &g);
+        if (le != cudaSuccess || ce != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return set_err(NE_ERR_CUDA, cudaGetErrorString(le != cudaSuccess ? le : ce));
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&w->gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) {
+            w->gexec = nullptr;
+            return set_err(NE_ERR_CUDA, cudaGetErrorString(ie));
+        }
+        w->gargs = a;
+        w->g_launches = L;
+        ++w->stats.graph_captures;
+    }
+    const uint32_t G = std::min(want, kGraphBatch);
+    neb::launch_batch_begin(w->d.ctl, w->stream);
+    ++w->launches;
+    for (uint32_t k = 0; k < G; ++k) NE_CUDA_TRY(cudaGraphLaunch(w->gexec, w->stream));
+    w->launches += (uint64_t)G * w->g_launches;
+    NE_CUDA_TRY(cudaMemcpyAsync(w->h_ctl, w->d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost, w->stream));
+    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
+    const neb::Ctl& c = *w->h_ctl;
+    *done = c.steps_done;
+    *halted = c.halt != 0;
+    w->stats.steps += c.steps_done;
+    w->stats.graph_steps += c.steps_done;
+    w->stats.epa_cap_hits += c.acc_epa;
+    if (!*halted) {
+        take_step_counts(w, c);
+        if (w->any_grid) {
+            const int kb = (((int)c.need_max + 7) / 8) * 8;
+            if (kb >= 8 && kb < w->key_bits) w->key_bits = kb;
+        }
+    }
+    if (c.acc_timeout) return set_err(NE_ERR_TIMEOUT, "a dataflow-solver dependency wait ran out");
+    if (c.acc_flags & 1u) *status = set_err(NE_ERR_NUMERIC, "an EPA or clipping budget was exceeded");
+    if (*halted) {
+        int rc;
+        if ((rc = restore_pre_step(w)) || (rc = grow_for(w, *w->h_ctl))) return rc;
+    }
+    return NE_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -801,73 +965,21 @@ int ne_world_step(NeWorld* w, uint32_t nsteps) {
     w->launches = 0;
     int status = NE_OK;
     if (w->n == 0) { w->stats.steps += nsteps; return NE_OK; }
-    for (uint32_t s = 0; s < nsteps; ++s) {
-        for (int attempt = 0;; ++attempt) {
-            if (attempt > 16) return set_err(NE_ERR_CAPACITY, "step did not fit after repeated growth");
-            neb::StepArgs a = make_args(w);
-            neb::launch_step(a, w->stream, &w->launches, w->profile ? w->ev : nullptr);
-            NE_CUDA_TRY(cudaGetLastError());
-            NE_CUDA_TRY(cudaMemcpyAsync(w->h_ctl, w->d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost, w->stream));
-            NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
-            const neb::Ctl& c = *w->h_ctl;
-            if (!c.abort) break;
-            // Restore the pre-step state and grow whatever overflowed.
-            const size_t bytes = (size_t)w->n * sizeof(neb::D4);
-            neb::DevWorld& d = w->d;
-            NE_CUDA_TRY(cudaMemcpyAsync(d.pos, d.s_pos, bytes, cudaMemcpyDeviceToDevice, w->stream));
-            NE_CUDA_TRY(cudaMemcpyAsync(d.quat, d.s_quat, bytes, cudaMemcpyDeviceToDevice, w->stream));
-            NE_CUDA_TRY(cudaMemcpyAsync(d.vel, d.s_vel, bytes, cudaMemcpyDeviceToDevice, w->stream));
-            NE_CUDA_TRY(cudaMemcpyAsync(d.omg, d.s_omg, bytes, cudaMemcpyDeviceToDevice, w->stream));
-            NE_CUDA_TRY(cudaMemcpyAsync(d.frc, d.s_frc, bytes, cudaMemcpyDeviceToDevice, w->stream));
-            NE_CUDA_TRY(cudaMemcpyAsync(d.trq, d.s_trq, bytes, cudaMemcpyDeviceToDevice, w->stream));
-            NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
-            int rc = NE_OK;
-            bool grew = false;
-            if ((int)c.need_bits > w->key_bits) {
-                w->key_bits = (((int)c.need_bits + 7) / 8) * 8;
-                grew = true;
-            }
-            if (c.P_ref > w->Rcap && (w->record & NE_RECORD_PAIRS)) {
-                if (c.P_ref > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 recorded pairs");
-                if ((rc = alloc_rec(w, grow_to(c.P_ref)))) return rc;
-                grew = true;
-            } else if (c.S > w->Scap) {
-                if (c.S > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 surviving pairs");
-                if ((rc = alloc_surv(w, grow_to(c.S)))) return rc;
-                grew = true;
-            } else if (c.C > w->Ccap) {
-                if (c.C > 0x7fffffffull) return set_err(NE_ERR_CAPACITY, "more than 2^31 contacts");
-                if ((rc = alloc_cons(w, grow_to(c.C)))) return rc;
-                grew = true;
-            }
-            if (!grew) return set_err(NE_ERR_CAPACITY, "step aborted without a growable cause");
-            if ((rc = alloc_scratch(w))) return rc;
-            ++w->stats.retries;
+    uint32_t s = 0;
+    while (s < nsteps) {
+        int rc;
+        if (graph_usable(w)) {
+            uint32_t done = 0;
+            bool halted = false;
+            if ((rc = step_graph_batch(w, nsteps - s, &done, &halted, &status))) return rc;
+            s += done;
+            if (!halted) continue;
+            // The batch stopped at a step that overflowed a buffer: that
+            // step's pre-step state is back in place and the buffer has
+            // grown; it is taken once more outside the graph.
         }
-        const neb::Ctl& c = *w->h_ctl;
-        if (w->profile) {
-            for (int k = 0; k < NE_NUM_STAGES; ++k) {
-                float ms = 0.f;
-                NE_CUDA_TRY(cudaEventElapsedTime(&ms, w->ev[k], w->ev[k + 1]));
-                w->stage_ms[k] += ms;
-            }
-            ++w->stage_steps;
-        }
-        // Shrink the cell-key sort to the bits this step needed.
-        if (w->any_grid) {
-            int kb = (((int)c.need_bits + 7) / 8) * 8;
-            if (kb >= 8) w->key_bits = kb;
-        }
-        w->stats.pairs = (w->record & NE_RECORD_PAIRS) ? c.P_ref : c.P;
-        w->stats.candidates = c.P;
-        w->stats.survivors = c.S;
-        w->stats.contacts = c.C;
-        w->stats.islands = c.islands;
-        w->stats.max_island = c.max_island;
-        w->stats.epa_cap_hits += c.epa_cap_hits;
-        w->stats.steps += 1;
-        if (c.solve_timeout) return set_err(NE_ERR_TIMEOUT, "a dataflow-solver dependency wait ran out");
-        if (c.flags & 1u) status = set_err(NE_ERR_NUMERIC, "an EPA or clipping budget was exceeded");
+        if ((rc = step_eager(w, &status))) return rc;
+        ++s;
     }
     return status;
 }
@@ -1329,6 +1441,12 @@ int ne_world_stream(const NeWorld* w, void** stream) {
 int ne_world_launch_count(const NeWorld* w, uint64_t* launches) {
     if (!w || !launches) return set_err(NE_ERR_ARG, "NULL argument");
     *launches = w->launches;
+    return NE_OK;
+}
+
+int ne_world_set_graph(NeWorld* w, int enable) {
+    if (!w) return set_err(NE_ERR_ARG, "world is NULL");
+    w->graph_on = enable != 0;
     return NE_OK;
 }
 

@@ -53,6 +53,16 @@ struct Ctl {
     uint64_t C2;             // 2 * C: rank entries of the dataflow solver
     uint64_t ncells;         // runs of equal cell keys after the sort (internal grid)
     uint64_t S_stage;        // surviving pairs staged so far this step
+    // Replayed batches of steps (CUDA graph): a step that aborts sets halt,
+    // and with StepArgs::sticky every later step of the batch is a no-op.
+    // The rest accumulates over the steps of a batch that completed.
+    uint32_t halt;
+    uint32_t steps_done;     // completed steps since the batch began
+    uint32_t acc_flags;      // OR of flags
+    uint32_t acc_timeout;    // OR of solve_timeout
+    uint32_t need_max;       // max of need_bits
+    uint32_t pad_;
+    uint64_t acc_epa;        // sum of epa_cap_hits
 };
 
 // Islands with at least kBigIsland contacts go to the team (dataflow)

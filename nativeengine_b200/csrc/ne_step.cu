@@ -216,7 +216,11 @@ __device__ __forceinline__ uint32_t upper_bound_u32(const uint32_t* a, uint32_t 
 
 // ---------------------------------------------------------------------------
 
-__global__ void k_step_begin(Ctl* ctl) {
+__global__ void k_step_begin(Ctl* ctl, int sticky) {
+    if (sticky && ctl->halt) {
+        ctl->abort = 1;   // an earlier step of this batch aborted: skip the step
+        return;
+    }
     ctl->abort = 0;
     ctl->flags = 0;
     ctl->need_bits = 0;
@@ -250,6 +254,7 @@ __global__ void __launch_bounds__(kT) k_integrate(StepArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const DevWorld& d = a.d;
+    if (d.ctl->abort) return;   // halted batch: the pre-step snapshot stays that of the aborted step
     const WorldP& W = a.wp[a.bw[i]];
     D4 p = d.pos[i], q4 = d.quat[i], v4 = d.vel[i], w4 = d.omg[i], f4 = d.frc[i], t4 = d.trq[i];
     d.s_pos[i] = p; d.s_quat[i] = q4; d.s_vel[i] = v4; d.s_omg[i] = w4; d.s_frc[i] = f4; d.s_trq[i] = t4;
@@ -1292,12 +1297,29 @@ __global__ void __launch_bounds__(kT) k_boundary(StepArgs a) {
 
 __global__ void k_step_end(StepArgs a) {
     Ctl* ctl = a.d.ctl;
-    if (ctl->abort) return;
+    if (ctl->abort) {
+        ctl->halt = 1;
+        return;
+    }
     if (a.warm) {
         const uint32_t nw = ctl->wsel ^ 1;
         ctl->wcount[nw] = (uint32_t)ctl->C;
         ctl->wsel = nw;
     }
+    ctl->steps_done += 1;
+    ctl->acc_flags |= ctl->flags;
+    ctl->acc_timeout |= ctl->solve_timeout;
+    ctl->need_max = max(ctl->need_max, ctl->need_bits);
+    ctl->acc_epa += ctl->epa_cap_hits;
+}
+
+__global__ void k_batch_begin(Ctl* ctl) {
+    ctl->halt = 0;
+    ctl->steps_done = 0;
+    ctl->acc_flags = 0;
+    ctl->acc_timeout = 0;
+    ctl->need_max = 0;
+    ctl->acc_epa = 0;
 }
 
 inline uint32_t blocks_for(uint64_t n, int t) { return (uint32_t)((n + t - 1) / t); }
@@ -1364,6 +1386,8 @@ void launch_big_prep(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launc
     *launches += 2;
 }
 
+void launch_batch_begin(Ctl* ctl, cudaStream_t st) { k_batch_begin<<<1, 1, 0, st>>>(ctl); }
+
 // Enqueue one step.  The host reads ctl afterwards to learn whether it must
 // be re-run with larger buffers.
 void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEvent_t* ev) {
@@ -1375,7 +1399,7 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
         if (ev) cudaEventRecord(ev[k], st);
     };
     mark(0);
-    k_step_begin<<<1, 1, 0, st>>>(ctl); ++L;
+    k_step_begin<<<1, 1, 0, st>>>(ctl, a.sticky); ++L;
     k_integrate<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
 
     mark(1);

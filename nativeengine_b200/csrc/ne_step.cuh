@@ -49,10 +49,16 @@ struct StepArgs {
     int big_threads;         // threads per CTA of the big-island solver (tuned)
     int big_ctas_per_sm;     // CTAs per SM of the big-island solver (tuned)
     int big_team_max;        // CTAs per big island: 1 = block-local solver, > 1 = team solver (tuned)
+    int sticky;              // replayed batch: an aborted step halts the rest of the batch
 };
 
 // ev: NE_NUM_STAGES + 1 events recorded at the stage boundaries, or nullptr.
+// Grid shapes depend on the capacities in a only (live counts are read on the
+// device), so the enqueued step can be captured once and replayed.
 void launch_step(const StepArgs& a, cudaStream_t st, uint64_t* launches, cudaEvent_t* ev);
+// Clears the batch fields of ctl (halt, steps_done, accumulators) before a
+// replayed batch of steps.
+void launch_batch_begin(Ctl* ctl, cudaStream_t st);
 
 // FP32 stages (ne_step_f32.cu), enqueued by launch_step when a.f32 is set;
 // the FP64 constraint build writes the FP32 solver records itself.

@@ -221,6 +221,10 @@ class DeviceWorld:
         _ffi.check(self._lib.ne_world_stream(self._h, C.byref(s)), "ne_world_stream")
         return s.value or 0
 
+    def set_graph(self, enable: bool) -> None:
+        """Steps by replaying a captured CUDA graph of one step (default on)."""
+        _ffi.check(self._lib.ne_world_set_graph(self._h, 1 if enable else 0), "ne_world_set_graph")
+
     def launch_count(self) -> int:
         v = C.c_uint64()
         _ffi.check(self._lib.ne_world_launch_count(self._h, C.byref(v)), "ne_world_launch_count")
