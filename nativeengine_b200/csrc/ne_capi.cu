@@ -177,7 +177,7 @@ void free_con_arrays(NeWorld* w) {
     dfree(d.con_imp); dfree(d.ilab[0]); dfree(d.ilab[1]); dfree(d.iord[0]); dfree(d.iord[1]); dfree(d.iflag);
     dfree(d.ioff); dfree(d.istart); dfree(d.big); dfree(d.con_kn);
     dfree(d.rkey[0]); dfree(d.rkey[1]); dfree(d.rval[0]); dfree(d.rval[1]); dfree(d.crank);
-    dfree(d.bcnt10); dfree(d.bq10); dfree(d.bctl); dfree(d.bteam);
+    dfree(d.bcnt10); dfree(d.bq10); dfree(d.bctl); dfree(d.bteam); dfree(d.brec);
     free_f32_cons(w);
 }
 
@@ -222,7 +222,8 @@ int alloc_cons(NeWorld* w, uint64_t cap) {
         (rc = dalloc(&d.rkey[1], 2 * cap)) || (rc = dalloc(&d.rval[0], 2 * cap)) ||
         (rc = dalloc(&d.rval[1], 2 * cap)) || (rc = dalloc(&d.crank, 2 * cap)) ||
         (rc = dalloc(&d.bcnt10, 10 * cap)) || (rc = dalloc(&d.bq10, 10 * cap)) ||
-        (rc = dalloc(&d.bctl, cap / neb::kBigIsland + 1)) || (rc = dalloc(&d.bteam, cap / neb::kBigIsland + 2)))
+        (rc = dalloc(&d.bctl, cap / neb::kBigIsland + 1)) || (rc = dalloc(&d.bteam, cap / neb::kBigIsland + 2)) ||
+        (rc = dalloc(&d.brec, 2 * cap)))
         return rc;
     if (w->precision == NE_PRECISION_F32 && (rc = alloc_f32_cons(w, cap))) return rc;
     unsigned long long* nk[2] = {nullptr, nullptr};
@@ -272,6 +273,7 @@ neb::StepArgs make_args(const NeWorld* w) {
     a.Ccap = w->Ccap;
     a.Rcap = w->Rcap;
     a.num_sms = w->num_sms;
+    a.local_cap = neb::kLocalCap;
     return a;
 }
 
@@ -456,6 +458,8 @@ int ne_world_create(const NeWorldParams* params, NeWorld** out) {
     NE_CUDA_TRY(cudaGetDevice(&w->device));
     NE_CUDA_TRY(cudaDeviceGetAttribute(&w->num_sms, cudaDevAttrMultiProcessorCount, w->device));
     NE_CUDA_TRY(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+    neb::init_kernel_attrs();
+    NE_CUDA_TRY(cudaGetLastError());
     NE_CUDA_TRY(cudaMallocHost((void**)&w->h_ctl, sizeof(neb::Ctl)));
     if ((rc = dalloc(&w->d.ctl, 1))) { ne_world_destroy(w); return rc; }
     std::memset(w->h_ctl, 0, sizeof(neb::Ctl));

@@ -131,6 +131,7 @@ struct DevWorld {
     uint32_t* bq10;          // [10C] ready queues of the solver updates
     BigCtl* bctl;            // [C/48 + 1] per big island
     uint32_t* bteam;         // [C/48 + 2] first virtual CTA of each big island's team
+    uint4* brec;             // [2C] per island position: {c, i, j, flags}, {next on i, next on j} (big islands)
     // batched FP32 form (null in FP64 mode): FP32 copies of the body state the
     // narrowphase and the solver read, refreshed every step after integration,
     // and the FP32 constraint records.  Poses, the warm-start impulses and the

@@ -147,9 +147,11 @@ __device__ __forceinline__ void island_solve_local(const StepArgs& a, int ib, in
     double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
     const uint32_t nbig = ctl->nbig;
     for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+        if (*(volatile uint32_t*)&ctl->solve_timeout) break;   // a wait ran out: stop, the step is an error
         const uint32_t t = d.big[bi];
         const uint32_t s = d.istart[t], e = d.istart[t + 1];
         const uint32_t m = e - s;
+        if (m <= a.local_cap) continue;          // island_solve_shared takes it
         const uint32_t total = 10u * m;
         const double beta = a.wp[a.bw[d.ci[ord[s]]]].beta;
         uint32_t* cnt = d.bcnt10 + 10u * s;      // per-island slices of the 10*C scratch
@@ -209,6 +211,183 @@ __device__ __forceinline__ void island_solve_local(const StepArgs& a, int ib, in
                 }
                 break;
             }
+        }
+        __syncthreads();
+    }
+}
+
+// ---- big islands: shared-memory dataflow solver (one CTA per island) -------
+//
+// The same update sequence and dependency rule as island_solve_local, with
+// the bookkeeping taken off the critical path:
+//
+//  * big_rec (a grid-wide pass before the solve) writes one 32-byte record
+//    per island position -- contact, bodies, mutability, phase-0 predecessor
+//    count, and the island position of the next update on each body (same
+//    phase, or bit 31 set: the body's first contact in the next phase) -- and
+//    empties the island's queue slots.  An update then costs one record load
+//    instead of a chain of index loads.
+//  * Predecessor counters are bytes in shared memory, one per contact
+//    position, reused by the ten phases: the update (p, q) re-arms its own
+//    counter for (p + 1, q) before it notifies anyone.  Every predecessor of
+//    (p + 1, q) comes after (p, q) on its body, so its decrement is ordered
+//    after that re-arm through the acquire/release chain of the counters.
+//    Four counters share a 32-bit word; a decrement never takes a byte below
+//    zero, so there is no borrow between them.
+//  * The lane whose decrement makes an update ready runs it next itself (a
+//    continuation); only a second ready successor goes through the queue.
+//
+// Islands above local_cap contacts are left to island_solve_local.
+__device__ __forceinline__ void big_rec(const StepArgs& a, int ib, int rb) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const DevWorld& d = a.d;
+    const uint64_t C = ctl->C;
+    const uint32_t* ord = d.iord[ib];
+    const uint32_t* rv = d.rval[rb];
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < C; k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = d.ioff[k] + d.iflag[k] - 1u;
+        const uint32_t s = d.istart[t], e = d.istart[t + 1];
+        if (e - s < kBigIsland) continue;
+        const uint32_t c = ord[k];
+        const uint32_t i = d.ci[c], j = d.cj[c];
+        const bool mi = (d.meta[i].y & kFlagMutable) != 0, mj = (d.meta[j].y & kFlagMutable) != 0;
+        uint32_t nxt[2] = {kEmpty, kEmpty}, npred0 = 0;
+        #pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            if (!(side ? mj : mi)) continue;
+            const uint32_t b = side ? j : i;
+            const uint32_t r = d.crank[2 * k + side];
+            const uint32_t deg = d.bdeg[b], base = d.bstart[b];
+            if (r != 0) ++npred0;
+            nxt[side] = (r + 1 < deg) ? (rv[base + r + 1] >> 1) - s : (((rv[base] >> 1) - s) | 0x80000000u);
+        }
+        d.brec[2 * k] = make_uint4(c, i, j, (mi ? 1u : 0u) | (mj ? 2u : 0u) | (npred0 << 2));
+        d.brec[2 * k + 1] = make_uint4(nxt[0], nxt[1], 0u, 0u);
+        uint32_t* q = d.bq10 + 10 * k;
+        #pragma unroll
+        for (int r = 0; r < 10; ++r) q[r] = kEmpty;
+    }
+}
+
+template <class Items>
+__device__ __forceinline__ void island_solve_shared(const StepArgs& a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    extern __shared__ uint32_t s_cnt[];   // a.local_cap byte counters
+    __shared__ uint32_t s_head, s_tail, s_done;
+    __shared__ int s_fail;
+    const DevWorld& d = a.d;
+    double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
+    const uint32_t nbig = ctl->nbig;
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    constexpr uint32_t kNone = 0xfffffffeu;
+    using BlockAtomic = cuda::atomic_ref<uint32_t, cuda::thread_scope_block>;
+    for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+        if (*(volatile uint32_t*)&ctl->solve_timeout) break;   // a wait ran out: stop, the step is an error
+        const uint32_t t = d.big[bi];
+        const uint32_t s = d.istart[t], e = d.istart[t + 1];
+        const uint32_t m = e - s;
+        if (m > a.local_cap) continue;
+        const uint32_t total = 10u * m;
+        const uint4* rec = d.brec + 2 * (size_t)s;
+        uint32_t* queue = d.bq10 + 10 * (size_t)s;
+        const double beta = a.wp[a.bw[rec[0].y]].beta;
+        if (threadIdx.x == 0) { s_head = 0; s_tail = 0; s_done = 0; s_fail = 0; }
+        for (uint32_t wd = threadIdx.x; 4 * wd < m; wd += blockDim.x) {
+            uint32_t word = 0;
+            #pragma unroll
+            for (int b = 0; b < 4; ++b)
+                if (4 * wd + b < m) word |= ((rec[2 * (4 * wd + b)].w >> 2) & 3u) << (8 * b);
+            s_cnt[wd] = word;
+        }
+        __syncthreads();
+        for (uint32_t q = threadIdx.x; q < m; q += blockDim.x)
+            if (((s_cnt[q >> 2] >> (8 * (q & 3))) & 0xffu) == 0u) {
+                BlockAtomic tl(s_tail);
+                BlockAtomic(queue[tl.fetch_add(1u, cuda::memory_order_relaxed)]).store(q, cuda::memory_order_relaxed);
+            }
+        __syncthreads();
+
+        BlockAtomic head(s_head), tail(s_tail), done(s_done);
+        uint32_t cont = kEmpty, slot = kNone;
+        unsigned long long last_progress = global_ns();
+        uint32_t rounds = 0;
+        while (true) {
+            // Lanes without work claim the next queue slots (one atomic per warp).
+            const bool need = cont == kEmpty && slot == kNone;
+            const uint32_t nb = __ballot_sync(0xffffffffu, need);
+            if (nb) {
+                uint32_t base = 0;
+                if (lane == __ffs(nb) - 1) base = head.fetch_add((uint32_t)__popc(nb), cuda::memory_order_relaxed);
+                base = __shfl_sync(0xffffffffu, base, __ffs(nb) - 1);
+                if (need) slot = base + __popc(nb & lt);
+            }
+            uint32_t u = cont;
+            cont = kEmpty;
+            if (u == kEmpty && slot < total) {
+                const uint32_t x = BlockAtomic(queue[slot]).load(cuda::memory_order_acquire);
+                if (x != kEmpty) { u = x; slot = kNone; }
+            }
+            const bool ready = u != kEmpty;
+            if (ready) {
+                const uint32_t p = u / m, q = u - p * m;
+                const uint4 r0 = rec[2 * q], r1 = rec[2 * q + 1];
+                if (p == 0) {
+                    if (a.warm) Items::warm(d, r0.x);
+                } else if (p <= 8) {
+                    Items::sweep(d, r0.x);
+                } else {
+                    Items::correct(d, r0.x, beta, wout);
+                }
+                const uint32_t sh = 8u * (q & 3u);
+                if (p < 9) BlockAtomic(s_cnt[q >> 2]).fetch_add(((r0.w & 1u) + ((r0.w >> 1) & 1u)) << sh,
+                                                                  cuda::memory_order_relaxed);
+                #pragma unroll
+                for (int side = 0; side < 2; ++side) {
+                    const uint32_t nx = side ? r1.y : r1.x;
+                    if (nx == kEmpty) continue;
+                    uint32_t np = p, nq = nx;
+                    if (nx & 0x80000000u) {
+                        if (p == 9) continue;
+                        np = p + 1;
+                        nq = nx & 0x7fffffffu;
+                    }
+                    const uint32_t nsh = 8u * (nq & 3u);
+                    const uint32_t old = BlockAtomic(s_cnt[nq >> 2]).fetch_sub(1u << nsh, cuda::memory_order_acq_rel);
+                    if (((old >> nsh) & 0xffu) != 1u) continue;
+                    const uint32_t nu = np * m + nq;
+                    if (cont == kEmpty) {
+                        cont = nu;
+                    } else {
+                        const uint32_t sl = tail.fetch_add(1u, cuda::memory_order_relaxed);
+                        BlockAtomic(queue[sl]).store(nu, cuda::memory_order_release);
+                    }
+                }
+            }
+            const uint32_t rb_ = __ballot_sync(0xffffffffu, ready);
+            if (rb_ && lane == __ffs(rb_) - 1) done.fetch_add((uint32_t)__popc(rb_), cuda::memory_order_relaxed);
+            if (rb_) {
+                rounds = 0;
+                last_progress = global_ns();
+                continue;
+            }
+            if (__any_sync(0xffffffffu, cont != kEmpty)) continue;
+            // Idle warp: finished island, failure elsewhere, or a stall.
+            ++rounds;   // warp-uniform
+            int stop = 0;
+            if (lane == 0) {
+                if (done.load(cuda::memory_order_relaxed) >= total) stop = 1;
+                else if (*(volatile int*)&s_fail) stop = 1;
+                else if ((rounds & 63u) == 0u && global_ns() - last_progress > kStallNs) stop = 2;
+            }
+            stop = __shfl_sync(0xffffffffu, stop, 0);
+            if (stop == 2 && lane == 0) {
+                s_fail = 1;
+                atomicExch(&ctl->solve_timeout, 1u);
+            }
+            if (stop) break;
         }
         __syncthreads();
     }

@@ -1256,6 +1256,12 @@ __global__ void __launch_bounds__(solve::kMaxBigThreads) k_island_solve_local(St
     solve::island_solve_local<ItemsF64<false>>(a, ib, rb);
 }
 
+__global__ void __launch_bounds__(256) k_big_rec(StepArgs a, int ib, int rb) { solve::big_rec(a, ib, rb); }
+
+__global__ void __launch_bounds__(solve::kMaxBigThreads) k_island_solve_shared(StepArgs a) {
+    solve::island_solve_shared<ItemsF64<false>>(a);
+}
+
 // wrapPositions() / applyWalls() (src/world.cpp:698-702, 635-657).
 __global__ void __launch_bounds__(kT) k_boundary(StepArgs a) {
     Ctl* ctl = a.d.ctl;
@@ -1311,6 +1317,7 @@ __global__ void k_step_end(StepArgs a) {
     ctl->acc_timeout |= ctl->solve_timeout;
     ctl->need_max = max(ctl->need_max, ctl->need_bits);
     ctl->acc_epa += ctl->epa_cap_hits;
+    if (ctl->solve_timeout) ctl->halt = 1;   // a failed solve ends a replayed batch
 }
 
 __global__ void k_batch_begin(Ctl* ctl) {
@@ -1387,6 +1394,16 @@ void launch_big_prep(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launc
 }
 
 void launch_batch_begin(Ctl* ctl, cudaStream_t st) { k_batch_begin<<<1, 1, 0, st>>>(ctl); }
+
+void launch_big_rec(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches) {
+    k_big_rec<<<a.num_sms * 8, 256, 0, st>>>(a, ib, rb);
+    ++*launches;
+}
+
+void init_kernel_attrs() {
+    cudaFuncSetAttribute(k_island_solve_shared, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLocalCap);
+    init_kernel_attrs_f32();
+}
 
 // Enqueue one step.  The host reads ctl afterwards to learn whether it must
 // be re-run with larger buffers.
@@ -1471,6 +1488,8 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
     } else {
         k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib); ++L;
         if (a.big_team_max == 1) {
+            launch_big_rec(a, ib, rb, st, launches);
+            k_island_solve_shared<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, a.local_cap, st>>>(a); ++L;
             k_island_solve_local<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb); ++L;
         } else {
             launch_big_prep(a, ib, st, launches);

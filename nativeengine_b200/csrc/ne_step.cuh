@@ -50,7 +50,15 @@ struct StepArgs {
     int big_ctas_per_sm;     // CTAs per SM of the big-island solver (tuned)
     int big_team_max;        // CTAs per big island: 1 = block-local solver, > 1 = team solver (tuned)
     int sticky;              // replayed batch: an aborted step halts the rest of the batch
+    uint32_t local_cap;      // big islands up to this many contacts: shared-memory dataflow solver
 };
+
+// Contacts per island the shared-memory dataflow solver takes (one counter
+// byte each: 64 KiB of dynamic shared memory per CTA).
+constexpr uint32_t kLocalCap = 65536;
+// Opt-in shared-memory sizes of the solver kernels (once per device).
+void init_kernel_attrs();
+void init_kernel_attrs_f32();
 
 // ev: NE_NUM_STAGES + 1 events recorded at the stage boundaries, or nullptr.
 // Grid shapes depend on the capacities in a only (live counts are read on the
@@ -66,6 +74,8 @@ void launch_narrowphase_f32(const StepArgs& a, cudaStream_t st, uint64_t* launch
 void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches);
 // Teams and dataflow state of the big islands (ne_step.cu; both precisions).
 void launch_big_prep(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launches);
+// Per-position records of the big islands for the shared-memory solver.
+void launch_big_rec(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches);
 // State transfer in the C-ABI's host layout: x[3n] | q[4n] | v[3n] | w[3n] |
 // force[3n] | torque[3n] (mask bit k = array k) to and from the records.
 void launch_unpack_state(const DevWorld& d, uint32_t n, const double* io, uint32_t mask, cudaStream_t st);

@@ -228,6 +228,10 @@ __global__ void __launch_bounds__(solve::kMaxBigThreads) k_island_solve_local_f3
     solve::island_solve_local<ItemsF32<false>>(a, ib, rb);
 }
 
+__global__ void __launch_bounds__(solve::kMaxBigThreads) k_island_solve_shared_f32(StepArgs a) {
+    solve::island_solve_shared<ItemsF32<false>>(a);
+}
+
 // Solver velocities back into the FP64 state: v64 += v32 - fl(v64).
 __global__ void __launch_bounds__(kT) k_writeback_f32(StepArgs a) {
     Ctl* ctl = a.d.ctl;
@@ -261,13 +265,20 @@ void launch_narrowphase_f32(const StepArgs& a, cudaStream_t st, uint64_t* launch
 void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches) {
     k_island_solve_f32<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib);
     if (a.big_team_max == 1) {
+        launch_big_rec(a, ib, rb, st, launches);
+        k_island_solve_shared_f32<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, a.local_cap, st>>>(a);
         k_island_solve_local_f32<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb);
+        ++*launches;
     } else {
         launch_big_prep(a, ib, st, launches);
         k_island_solve_big_f32<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb);
     }
     k_writeback_f32<<<blocks_for(a.n, kT), kT, 0, st>>>(a);
     *launches += 3;
+}
+
+void init_kernel_attrs_f32() {
+    cudaFuncSetAttribute(k_island_solve_shared_f32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLocalCap);
 }
 
 void convert_verts_f32(const D4* src, F4* dst, uint32_t count, cudaStream_t st) {
