@@ -495,7 +495,7 @@ def run_ours(args):
                        "step_launch": "CUDA graph of the whole step, replayed once per step; one read of the "
                                       "device control block per step",
                        "graph_steps": stats["graph_steps"]},
-            "roofline": {"bound": "hbm", "kernel": "solve (k_island_solve + k_island_solve_local)",
+            "roofline": {"bound": "hbm", "kernel": "solve (k_island_solve + k_big_rec + k_island_solve_shared + k_island_solve_local)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": peak_kind, "traffic": profile_traffic(C_last),
                          "note": "latency-bound: the exact Gauss-Seidel order is a dependency chain; "

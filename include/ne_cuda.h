@@ -249,7 +249,7 @@ int ne_world_set_precision(NeWorld* world, int precision);
 
 /* Launch shape of the big-island solver (islands of >= 48 contacts).  No
  * counterpart in the reference.  Results do not depend on it.
- * threads: 128, 256 or 512 per CTA; ctas_per_sm: 1..4;
+ * threads: a multiple of 32 in 64..512 per CTA; ctas_per_sm: 1..4;
  * team_max: 1 = each big island is solved by one CTA (ready queue in shared
  * memory); 2..64 = an island may be solved by a team of up to team_max CTAs
  * on different SMs (queue and counters in global memory), sized in proportion

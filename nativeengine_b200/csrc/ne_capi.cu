@@ -1086,8 +1086,8 @@ int ne_world_set_precision(NeWorld* w, int precision) {
 
 int ne_world_set_solver_shape(NeWorld* w, const NeSolverShape* s) {
     if (!w || !s) return set_err(NE_ERR_ARG, "NULL argument");
-    if (s->threads != 128 && s->threads != 256 && s->threads != 512)
-        return set_err(NE_ERR_ARG, "solver threads must be 128, 256 or 512");
+    if (s->threads < 64 || s->threads > 512 || s->threads % 32 != 0)
+        return set_err(NE_ERR_ARG, "solver threads must be a multiple of 32 in 64..512");
     if (s->ctas_per_sm < 1 || s->ctas_per_sm > 4) return set_err(NE_ERR_ARG, "solver ctas_per_sm must be 1..4");
     if (s->team_max < 1 || s->team_max > 64) return set_err(NE_ERR_ARG, "solver team_max must be 1..64");
     w->big_threads = s->threads;

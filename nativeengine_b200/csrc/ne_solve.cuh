@@ -315,20 +315,43 @@ __device__ __forceinline__ void island_solve_shared(const StepArgs& a) {
         unsigned long long last_progress = global_ns();
         uint32_t rounds = 0;
         while (true) {
-            // Lanes without work claim the next queue slots (one atomic per warp).
+            // Lanes without work take queue entries that have been pushed
+            // (never slots ahead of the tail): an entry goes to the first warp
+            // with an idle lane that comes by, not to a lane whose warp is
+            // still busy with a long update.
             const bool need = cont == kEmpty && slot == kNone;
             const uint32_t nb = __ballot_sync(0xffffffffu, need);
             if (nb) {
-                uint32_t base = 0;
-                if (lane == __ffs(nb) - 1) base = head.fetch_add((uint32_t)__popc(nb), cuda::memory_order_relaxed);
+                uint32_t base = 0, take = 0;
+                if (lane == __ffs(nb) - 1) {
+                    uint32_t h = head.load(cuda::memory_order_relaxed);
+                    for (int tries = 0; tries < 8; ++tries) {
+                        const uint32_t avail = tail.load(cuda::memory_order_relaxed) - h;
+                        take = min((uint32_t)__popc(nb), avail);
+                        if (take == 0) break;
+                        if (head.compare_exchange_weak(h, h + take, cuda::memory_order_relaxed)) { base = h; break; }
+                        take = 0;
+                    }
+                }
                 base = __shfl_sync(0xffffffffu, base, __ffs(nb) - 1);
-                if (need) slot = base + __popc(nb & lt);
+                take = __shfl_sync(0xffffffffu, take, __ffs(nb) - 1);
+                const uint32_t rank = __popc(nb & lt);
+                if (need && rank < take) slot = base + rank;
             }
+            // Ordering: an update's stores and its counter re-arm are released
+            // by one fence before its notifications (relaxed counter
+            // decrements); the lane that takes a successor -- as its
+            // continuation, or from the queue -- fences once after seeing it
+            // ready, which acquires every predecessor's stores.
             uint32_t u = cont;
             cont = kEmpty;
             if (u == kEmpty && slot < total) {
-                const uint32_t x = BlockAtomic(queue[slot]).load(cuda::memory_order_acquire);
-                if (x != kEmpty) { u = x; slot = kNone; }
+                const uint32_t x = BlockAtomic(queue[slot]).load(cuda::memory_order_relaxed);
+                if (x != kEmpty) {
+                    u = x;
+                    slot = kNone;
+                    cuda::atomic_thread_fence(cuda::memory_order_acq_rel, cuda::thread_scope_block);
+                }
             }
             const bool ready = u != kEmpty;
             if (ready) {
@@ -342,8 +365,10 @@ __device__ __forceinline__ void island_solve_shared(const StepArgs& a) {
                     Items::correct(d, r0.x, beta, wout);
                 }
                 const uint32_t sh = 8u * (q & 3u);
-                if (p < 9) BlockAtomic(s_cnt[q >> 2]).fetch_add(((r0.w & 1u) + ((r0.w >> 1) & 1u)) << sh,
-                                                                  cuda::memory_order_relaxed);
+                if (p < 9) atomicAdd(&s_cnt[q >> 2], ((r0.w & 1u) + ((r0.w >> 1) & 1u)) << sh);
+                cuda::atomic_thread_fence(cuda::memory_order_acq_rel, cuda::thread_scope_block);
+                uint32_t extra = kEmpty;
+                bool got = false;
                 #pragma unroll
                 for (int side = 0; side < 2; ++side) {
                     const uint32_t nx = side ? r1.y : r1.x;
@@ -355,15 +380,16 @@ __device__ __forceinline__ void island_solve_shared(const StepArgs& a) {
                         nq = nx & 0x7fffffffu;
                     }
                     const uint32_t nsh = 8u * (nq & 3u);
-                    const uint32_t old = BlockAtomic(s_cnt[nq >> 2]).fetch_sub(1u << nsh, cuda::memory_order_acq_rel);
+                    const uint32_t old = atomicSub(&s_cnt[nq >> 2], 1u << nsh);
                     if (((old >> nsh) & 0xffu) != 1u) continue;
+                    got = true;
                     const uint32_t nu = np * m + nq;
-                    if (cont == kEmpty) {
-                        cont = nu;
-                    } else {
-                        const uint32_t sl = tail.fetch_add(1u, cuda::memory_order_relaxed);
-                        BlockAtomic(queue[sl]).store(nu, cuda::memory_order_release);
-                    }
+                    if (cont == kEmpty) cont = nu; else extra = nu;
+                }
+                if (got) cuda::atomic_thread_fence(cuda::memory_order_acq_rel, cuda::thread_scope_block);
+                if (extra != kEmpty) {
+                    const uint32_t sl = tail.fetch_add(1u, cuda::memory_order_relaxed);
+                    BlockAtomic(queue[sl]).store(extra, cuda::memory_order_relaxed);
                 }
             }
             const uint32_t rb_ = __ballot_sync(0xffffffffu, ready);

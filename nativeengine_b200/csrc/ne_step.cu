@@ -1166,75 +1166,93 @@ __device__ __forceinline__ void store_solver_body(const DevWorld& d, uint32_t i,
     solve::st_state<C>(d.omg + i, d4of(b.w, 0.0));
 }
 
+// The arithmetic of the three kinds of update on operands already loaded.
+// Warm-start application of one contact (src/world.cpp:560-567).
+__device__ __forceinline__ void warm_math(BodyS& A, BodyS& B, const D4& cn, const D4& ra4, const D4& rb4,
+                                          double nImp) {
+    apply_pair_impulse(A, B, v3of(ra4), v3of(rb4), v3of(cn) * nImp);
+}
+
+// One sequential-impulse update of one contact (src/world.cpp:575-610).  Kn
+// is the effMass along n computed once at constraint build: the reference
+// recomputes it every sweep from the same (unchanged) operands, so the value
+// is identical.
+__device__ __forceinline__ void sweep_math(BodyS& A, BodyS& B, const D4& cn, const D4& ra4, const D4& rb4,
+                                           double Kn, double2& imp) {
+    const V3 n = v3of(cn), rA = v3of(ra4), rB = v3of(rb4);
+    const double restBias = ra4.w, mu = rb4.w;
+    const V3 vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+    const double vn = dot(vc, n);
+    if (Kn > 1e-18) {
+        double dj = (restBias - vn) / Kn;
+        const double old = imp.x;
+        imp.x = (old + dj > 0.0) ? old + dj : 0.0;
+        dj = imp.x - old;
+        apply_pair_impulse(A, B, rA, rB, n * dj);
+    }
+    if (mu > 0.0 && imp.x > 0.0) {
+        const V3 vc2 = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+        const V3 vt = vc2 - n * dot(vc2, n);
+        const double vtl = norm(vt);
+        if (vtl > 1e-12) {
+            const V3 tg = vt / vtl;
+            const double Kt = eff_mass(A, B, rA, rB, tg);
+            if (Kt > 1e-18) {
+                double djt = -vtl / Kt;
+                const double maxF = mu * imp.x;
+                const double old = imp.y;
+                const double sum = old + djt;
+                imp.y = (sum < -maxF) ? -maxF : (sum > maxF ? maxF : sum);
+                djt = imp.y - old;
+                apply_pair_impulse(A, B, rA, rB, tg * djt);
+            }
+        }
+    }
+}
+
+// correctPenetration (src/contact.hpp:78-85): the position change of each
+// body (false = no change).
+__device__ __forceinline__ bool correct_math(const D4& pa, const D4& pb, const D4& cn, double beta, D4& na,
+                                             D4& nb) {
+    const double invSum = pa.w + pb.w;
+    const double overlap = cn.w;
+    if (invSum <= 0.0 || overlap <= 0.0) return false;
+    const V3 corr = v3of(cn) * (beta * overlap / invSum);
+    na = d4of(v3of(pa) + corr * pa.w, pa.w);
+    nb = d4of(v3of(pb) - corr * pb.w, pb.w);
+    return true;
+}
+
 template <bool C>
 struct ItemsF64 {
-    // Warm-start application of one contact (src/world.cpp:560-567).
     static __device__ __forceinline__ void warm(const DevWorld& d, uint32_t c) {
         const double nImp = solve::ld_state<C>(d.con_imp + c).x;
         if (nImp == 0.0) return;
         const uint32_t i = d.ci[c], j = d.cj[c];
         BodyS A = load_solver_body<C>(d, i), B = load_solver_body<C>(d, j);
-        const V3 n = v3of(d.con_n[c]), rA = v3of(d.con_ra[c]), rB = v3of(d.con_rb[c]);
-        apply_pair_impulse(A, B, rA, rB, n * nImp);
+        warm_math(A, B, d.con_n[c], d.con_ra[c], d.con_rb[c], nImp);
         store_solver_body<C>(d, i, A);
         store_solver_body<C>(d, j, B);
     }
 
-    // One sequential-impulse update of one contact (src/world.cpp:575-610).
-    // Kn is the effMass along n computed once at constraint build: the
-    // reference recomputes it every sweep from the same (unchanged) operands,
-    // so the value is identical.
     static __device__ __forceinline__ void sweep(const DevWorld& d, uint32_t c) {
         const uint32_t i = d.ci[c], j = d.cj[c];
         BodyS A = load_solver_body<C>(d, i), B = load_solver_body<C>(d, j);
-        const D4 cn = d.con_n[c], ra4 = d.con_ra[c], rb4 = d.con_rb[c];
-        const V3 n = v3of(cn), rA = v3of(ra4), rB = v3of(rb4);
-        const double restBias = ra4.w, mu = rb4.w;
-        const double Kn = d.con_kn[c];
         double2 imp = solve::ld_state<C>(d.con_imp + c);
-        const V3 vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
-        const double vn = dot(vc, n);
-        if (Kn > 1e-18) {
-            double dj = (restBias - vn) / Kn;
-            const double old = imp.x;
-            imp.x = (old + dj > 0.0) ? old + dj : 0.0;
-            dj = imp.x - old;
-            apply_pair_impulse(A, B, rA, rB, n * dj);
-        }
-        if (mu > 0.0 && imp.x > 0.0) {
-            const V3 vc2 = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
-            const V3 vt = vc2 - n * dot(vc2, n);
-            const double vtl = norm(vt);
-            if (vtl > 1e-12) {
-                const V3 tg = vt / vtl;
-                const double Kt = eff_mass(A, B, rA, rB, tg);
-                if (Kt > 1e-18) {
-                    double djt = -vtl / Kt;
-                    const double maxF = mu * imp.x;
-                    const double old = imp.y;
-                    const double sum = old + djt;
-                    imp.y = (sum < -maxF) ? -maxF : (sum > maxF ? maxF : sum);
-                    djt = imp.y - old;
-                    apply_pair_impulse(A, B, rA, rB, tg * djt);
-                }
-            }
-        }
+        sweep_math(A, B, d.con_n[c], d.con_ra[c], d.con_rb[c], d.con_kn[c], imp);
         solve::st_state<C>(d.con_imp + c, imp);
         store_solver_body<C>(d, i, A);
         store_solver_body<C>(d, j, B);
     }
 
-    // correctPenetration (src/contact.hpp:78-85) and the warm-cache store value.
+    // correctPenetration and the warm-cache store value.
     static __device__ __forceinline__ void correct(const DevWorld& d, uint32_t c, double beta, double* wimp_out) {
         const uint32_t i = d.ci[c], j = d.cj[c];
         const D4 pa = solve::ld_state<C>(d.pos + i), pb = solve::ld_state<C>(d.pos + j);
-        const double invSum = pa.w + pb.w;
-        const D4 cn = d.con_n[c];
-        const double overlap = cn.w;
-        if (!(invSum <= 0.0 || overlap <= 0.0)) {
-            const V3 corr = v3of(cn) * (beta * overlap / invSum);
-            if (d.meta[i].y & kFlagMutable) solve::st_state<C>(d.pos + i, d4of(v3of(pa) + corr * pa.w, pa.w));
-            if (d.meta[j].y & kFlagMutable) solve::st_state<C>(d.pos + j, d4of(v3of(pb) - corr * pb.w, pb.w));
+        D4 na, nb;
+        if (correct_math(pa, pb, d.con_n[c], beta, na, nb)) {
+            if (d.meta[i].y & kFlagMutable) solve::st_state<C>(d.pos + i, na);
+            if (d.meta[j].y & kFlagMutable) solve::st_state<C>(d.pos + j, nb);
         }
         if (wimp_out) wimp_out[c] = solve::ld_state<C>(d.con_imp + c).x;
     }

@@ -143,74 +143,89 @@ __device__ __forceinline__ void apply_pair_impulse_f32(BodyF& A, BodyF& B, const
     B.w = B.w - apply_inv_inertia(B.q, B.invI, cross(rb, J));
 }
 
+// The arithmetic of the three kinds of update on operands already loaded.
+// Warm-start application (src/world.cpp:560-567).
+__device__ __forceinline__ void warm_math_f32(BodyF& A, BodyF& B, const F4& n4, const F4& ra4, const F4& rb4,
+                                              double nImp) {
+    apply_pair_impulse_f32(A, B, v3f(ra4), v3f(rb4), v3f(n4) * (float)nImp);
+}
+
+// One sequential-impulse update (src/world.cpp:575-610).  nImp accumulates
+// in FP64; the velocity change it implies is FP32.
+__device__ __forceinline__ void sweep_math_f32(BodyF& A, BodyF& B, const F4& n4, const F4& ra4, const F4& rb4,
+                                               float Kn, double2& imp) {
+    const V3f n = v3f(n4), rA = v3f(ra4), rB = v3f(rb4);
+    const float restBias = ra4.w, mu = rb4.w;
+    const V3f vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+    const float vn = dot(vc, n);
+    if (Kn > 1e-18f) {
+        const float dj = (restBias - vn) / Kn;
+        const double old = imp.x;
+        const double sum = old + (double)dj;
+        imp.x = (sum > 0.0) ? sum : 0.0;
+        apply_pair_impulse_f32(A, B, rA, rB, n * (float)(imp.x - old));
+    }
+    if (mu > 0.0f && imp.x > 0.0) {
+        const V3f vc2 = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
+        const V3f vt = vc2 - n * dot(vc2, n);
+        const float vtl = norm(vt);
+        if (vtl > 1e-12f) {
+            const V3f tg = vt / vtl;
+            const float Kt = eff_mass_f32(A, B, rA, rB, tg);
+            if (Kt > 1e-18f) {
+                const float djt = -vtl / Kt;
+                const float maxF = mu * (float)imp.x;
+                const float old = (float)imp.y;
+                const float sum = old + djt;
+                const float nt = (sum < -maxF) ? -maxF : (sum > maxF ? maxF : sum);
+                imp.y = (double)nt;
+                apply_pair_impulse_f32(A, B, rA, rB, tg * (nt - old));
+            }
+        }
+    }
+}
+
+// correctPenetration (src/contact.hpp:78-85): FP32 displacement, FP64 pose.
+__device__ __forceinline__ bool correct_math_f32(const D4& pa, const D4& pb, const F4& n4, double beta, D4& na,
+                                                 D4& nb) {
+    const float invSum = (float)pa.w + (float)pb.w;
+    const float overlap = n4.w;
+    if (invSum <= 0.0f || overlap <= 0.0f) return false;
+    const V3f corr = v3f(n4) * ((float)beta * overlap / invSum);
+    na = d4of(v3d(pa) + cvt<double>(corr * (float)pa.w), pa.w);
+    nb = d4of(v3d(pb) - cvt<double>(corr * (float)pb.w), pb.w);
+    return true;
+}
+
 template <bool C>
 struct ItemsF32 {
-    // Warm-start application (src/world.cpp:560-567).
     static __device__ __forceinline__ void warm(const DevWorld& d, uint32_t c) {
         const double nImp = solve::ld_state<C>(d.con_imp + c).x;
         if (nImp == 0.0) return;
         const uint32_t i = d.ci[c], j = d.cj[c];
         BodyF A = load_body_f32<C>(d, i), B = load_body_f32<C>(d, j);
-        apply_pair_impulse_f32(A, B, v3f(d.f_ra[c]), v3f(d.f_rb[c]), v3f(d.f_n[c]) * (float)nImp);
+        warm_math_f32(A, B, d.f_n[c], d.f_ra[c], d.f_rb[c], nImp);
         store_body_f32<C>(d, i, A);
         store_body_f32<C>(d, j, B);
     }
 
-    // One sequential-impulse update (src/world.cpp:575-610).  nImp
-    // accumulates in FP64; the velocity change it implies is FP32.
     static __device__ __forceinline__ void sweep(const DevWorld& d, uint32_t c) {
         const uint32_t i = d.ci[c], j = d.cj[c];
         BodyF A = load_body_f32<C>(d, i), B = load_body_f32<C>(d, j);
-        const F4 ra4 = d.f_ra[c], rb4 = d.f_rb[c];
-        const V3f n = v3f(d.f_n[c]), rA = v3f(ra4), rB = v3f(rb4);
-        const float restBias = ra4.w, mu = rb4.w;
-        const float Kn = d.f_kn[c];
         double2 imp = solve::ld_state<C>(d.con_imp + c);
-        const V3f vc = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
-        const float vn = dot(vc, n);
-        if (Kn > 1e-18f) {
-            const float dj = (restBias - vn) / Kn;
-            const double old = imp.x;
-            const double sum = old + (double)dj;
-            imp.x = (sum > 0.0) ? sum : 0.0;
-            apply_pair_impulse_f32(A, B, rA, rB, n * (float)(imp.x - old));
-        }
-        if (mu > 0.0f && imp.x > 0.0) {
-            const V3f vc2 = (A.v + cross(A.w, rA)) - (B.v + cross(B.w, rB));
-            const V3f vt = vc2 - n * dot(vc2, n);
-            const float vtl = norm(vt);
-            if (vtl > 1e-12f) {
-                const V3f tg = vt / vtl;
-                const float Kt = eff_mass_f32(A, B, rA, rB, tg);
-                if (Kt > 1e-18f) {
-                    const float djt = -vtl / Kt;
-                    const float maxF = mu * (float)imp.x;
-                    const float old = (float)imp.y;
-                    const float sum = old + djt;
-                    const float nt = (sum < -maxF) ? -maxF : (sum > maxF ? maxF : sum);
-                    imp.y = (double)nt;
-                    apply_pair_impulse_f32(A, B, rA, rB, tg * (nt - old));
-                }
-            }
-        }
+        sweep_math_f32(A, B, d.f_n[c], d.f_ra[c], d.f_rb[c], d.f_kn[c], imp);
         solve::st_state<C>(d.con_imp + c, imp);
         store_body_f32<C>(d, i, A);
         store_body_f32<C>(d, j, B);
     }
 
-    // correctPenetration (src/contact.hpp:78-85): FP32 displacement, FP64 pose.
     static __device__ __forceinline__ void correct(const DevWorld& d, uint32_t c, double beta, double* wout) {
         const uint32_t i = d.ci[c], j = d.cj[c];
         const D4 pa = solve::ld_state<C>(d.pos + i), pb = solve::ld_state<C>(d.pos + j);
-        const float invSum = (float)pa.w + (float)pb.w;
-        const F4 n4 = d.f_n[c];
-        const float overlap = n4.w;
-        if (!(invSum <= 0.0f || overlap <= 0.0f)) {
-            const V3f corr = v3f(n4) * ((float)beta * overlap / invSum);
-            if (d.meta[i].y & kFlagMutable)
-                solve::st_state<C>(d.pos + i, d4of(v3d(pa) + cvt<double>(corr * (float)pa.w), pa.w));
-            if (d.meta[j].y & kFlagMutable)
-                solve::st_state<C>(d.pos + j, d4of(v3d(pb) - cvt<double>(corr * (float)pb.w), pb.w));
+        D4 na, nb;
+        if (correct_math_f32(pa, pb, d.f_n[c], beta, na, nb)) {
+            if (d.meta[i].y & kFlagMutable) solve::st_state<C>(d.pos + i, na);
+            if (d.meta[j].y & kFlagMutable) solve::st_state<C>(d.pos + j, nb);
         }
         if (wout) wout[c] = solve::ld_state<C>(d.con_imp + c).x;
     }
