@@ -253,7 +253,9 @@ int ne_world_set_precision(NeWorld* world, int precision);
  * team_max: 1 = each big island is solved by one CTA (ready queue in shared
  * memory); 2..64 = an island may be solved by a team of up to team_max CTAs
  * on different SMs (queue and counters in global memory), sized in proportion
- * to its share of the work.
+ * to its share of the work.  Until set or tuned, the shape follows the last
+ * upload: 384 threads x 1 CTA per SM for a single world, 128 x 3 for a
+ * batch of several worlds.
  * ne_world_autotune times each candidate shape for `steps` steps from the
  * current state, keeps the fastest and restores the state and warm cache, so
  * the world continues as if it had not been called; *chosen (may be NULL)

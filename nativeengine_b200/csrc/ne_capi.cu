@@ -82,9 +82,10 @@ struct NeWorld {
     std::vector<uint8_t> h_large;         // body flagged large (internal grid)
     uint32_t record = 0;                  // NE_RECORD_* flags
     int precision = NE_PRECISION_F64;
-    uint32_t big_threads = 512;           // big-island solver launch shape
+    uint32_t big_threads = 384;           // big-island solver launch shape
     uint32_t big_ctas_per_sm = 1;
     uint32_t big_team_max = 1;
+    bool shape_chosen = false;            // set by the caller or the autotuner (else per upload)
     size_t nverts = 0;                    // convex vertex pool entries on the device
     uint64_t Rcap = 0;                    // capacity of the recorded pair list
     int key_bits = 64;
@@ -177,7 +178,7 @@ void free_con_arrays(NeWorld* w) {
     dfree(d.con_imp); dfree(d.ilab[0]); dfree(d.ilab[1]); dfree(d.iord[0]); dfree(d.iord[1]); dfree(d.iflag);
     dfree(d.ioff); dfree(d.istart); dfree(d.big); dfree(d.con_kn);
     dfree(d.rkey[0]); dfree(d.rkey[1]); dfree(d.rval[0]); dfree(d.rval[1]); dfree(d.crank);
-    dfree(d.bcnt10); dfree(d.bq10); dfree(d.bctl); dfree(d.bteam); dfree(d.brec);
+    dfree(d.bcnt10); dfree(d.bq10); dfree(d.bctl); dfree(d.bteam); dfree(d.brec); dfree(d.bigs);
     free_f32_cons(w);
 }
 
@@ -223,7 +224,7 @@ int alloc_cons(NeWorld* w, uint64_t cap) {
         (rc = dalloc(&d.rval[1], 2 * cap)) || (rc = dalloc(&d.crank, 2 * cap)) ||
         (rc = dalloc(&d.bcnt10, 10 * cap)) || (rc = dalloc(&d.bq10, 10 * cap)) ||
         (rc = dalloc(&d.bctl, cap / neb::kBigIsland + 1)) || (rc = dalloc(&d.bteam, cap / neb::kBigIsland + 2)) ||
-        (rc = dalloc(&d.brec, 2 * cap)))
+        (rc = dalloc(&d.brec, 2 * cap)) || (rc = dalloc(&d.bigs, cap / neb::kBigIsland + 1)))
         return rc;
     if (w->precision == NE_PRECISION_F32 && (rc = alloc_f32_cons(w, cap))) return rc;
     unsigned long long* nk[2] = {nullptr, nullptr};
@@ -671,6 +672,15 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
 
     w->nworlds = nworlds;
     w->wparams.assign(params, params + nworlds);
+    // Default solver shape until the caller sets or tunes one: one island
+    // per SM in one wide CTA for a single world (its big island is a long
+    // dependency chain), several narrower CTAs per SM for a batch (many
+    // islands of a few hundred to a few thousand contacts).
+    if (!w->shape_chosen) {
+        w->big_threads = nworlds > 1 ? 128 : 384;
+        w->big_ctas_per_sm = nworlds > 1 ? 3 : 1;
+        w->big_team_max = 1;
+    }
     w->wbegin.assign(wbegin, wbegin + nworlds + 1);
     w->h_bound = boundR;
     w->h_shape = shapes;
@@ -1093,6 +1103,7 @@ int ne_world_set_solver_shape(NeWorld* w, const NeSolverShape* s) {
     w->big_threads = s->threads;
     w->big_ctas_per_sm = s->ctas_per_sm;
     w->big_team_max = s->team_max;
+    w->shape_chosen = true;
     return NE_OK;
 }
 
@@ -1364,10 +1375,15 @@ int ne_world_autotune(NeWorld* w, uint32_t steps, NeSolverShape* chosen) {
     NE_CUDA_TRY(cudaSetDevice(w->device));
     NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
     if (steps == 0) steps = 1;
-    static const NeSolverShape cand[] = {{512, 1, 1}, {256, 1, 1}, {256, 2, 1}, {128, 1, 1}, {128, 2, 1},
-                                         {128, 4, 1}, {256, 1, 4}, {256, 1, 16}, {128, 2, 8}};
+    static const NeSolverShape cand[] = {{512, 1, 1}, {384, 1, 1}, {256, 1, 1}, {256, 2, 1}, {128, 1, 1},
+                                         {128, 2, 1}, {128, 3, 1}, {64, 3, 1}, {256, 1, 4}, {256, 1, 16},
+                                         {128, 2, 8}};
     const bool prof = w->profile;
     w->profile = false;
+    // Candidates change the launch shape, so each would re-capture the step
+    // graph inside its timing: time them kernel by kernel instead.
+    const bool graph = w->graph_on;
+    w->graph_on = false;
     Saved s;
     int rc = save_state(w, s);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -1395,7 +1411,9 @@ int ne_world_autotune(NeWorld* w, uint32_t steps, NeSolverShape* chosen) {
     w->big_threads = best.threads;
     w->big_ctas_per_sm = best.ctas_per_sm;
     w->big_team_max = best.team_max;
+    if (rc == NE_OK) w->shape_chosen = true;
     w->profile = prof;
+    w->graph_on = graph;
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     saved_free(s);

@@ -63,6 +63,12 @@ struct Ctl {
     uint32_t need_max;       // max of need_bits
     uint32_t pad_;
     uint64_t acc_epa;        // sum of epa_cap_hits
+    // Big islands in claim order for the shared-memory solver: counts per
+    // size class (floor(log2 contacts)), fill cursors, and the claim counter.
+    uint32_t big_class[32];
+    uint32_t big_fill[32];
+    uint32_t big_next;
+    uint32_t pad2_;
 };
 
 // Islands with at least kBigIsland contacts go to the team (dataflow)
@@ -131,6 +137,7 @@ struct DevWorld {
     uint32_t* bq10;          // [10C] ready queues of the solver updates
     BigCtl* bctl;            // [C/48 + 1] per big island
     uint32_t* bteam;         // [C/48 + 2] first virtual CTA of each big island's team
+    uint32_t* bigs;          // [C/48 + 1] big islands, larger size classes first
     uint4* brec;             // [2C] per island position: {c, i, j, flags}, {next on i, next on j} (big islands)
     // batched FP32 form (null in FP64 mode): FP32 copies of the body state the
     // narrowphase and the solver read, refreshed every step after integration,

@@ -93,6 +93,7 @@ __device__ __forceinline__ void island_solve_small(const StepArgs& a, int ib) {
     if (e - s >= kBigIsland) {
         const uint32_t slot = atomicAdd(&ctl->nbig, 1u);
         d.big[slot] = (uint32_t)t;
+        atomicAdd(&ctl->big_class[31 - __clz(e - s)], 1u);
         return;
     }
     const uint32_t* ord = d.iord[ib];
@@ -146,12 +147,15 @@ __device__ __forceinline__ void island_solve_local(const StepArgs& a, int ib, in
     const uint32_t* rv = d.rval[rb];
     double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
     const uint32_t nbig = ctl->nbig;
+    __shared__ uint32_t s_stop;
     for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
-        if (*(volatile uint32_t*)&ctl->solve_timeout) break;   // a wait ran out: stop, the step is an error
         const uint32_t t = d.big[bi];
         const uint32_t s = d.istart[t], e = d.istart[t + 1];
         const uint32_t m = e - s;
         if (m <= a.local_cap) continue;          // island_solve_shared takes it
+        if (threadIdx.x == 0) s_stop = *(volatile uint32_t*)&ctl->solve_timeout;
+        __syncthreads();
+        if (s_stop) break;                       // a wait ran out elsewhere: the step is an error
         const uint32_t total = 10u * m;
         const double beta = a.wp[a.bw[d.ci[ord[s]]]].beta;
         uint32_t* cnt = d.bcnt10 + 10u * s;      // per-island slices of the 10*C scratch
@@ -245,6 +249,15 @@ __device__ __forceinline__ void big_rec(const StepArgs& a, int ib, int rb) {
     const uint64_t C = ctl->C;
     const uint32_t* ord = d.iord[ib];
     const uint32_t* rv = d.rval[rb];
+    // Claim order of the big islands: larger size classes first.
+    const uint32_t nbig = ctl->nbig;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < nbig; g += gridDim.x * blockDim.x) {
+        const uint32_t t = d.big[g];
+        const uint32_t cls = 31 - __clz(d.istart[t + 1] - d.istart[t]);
+        uint32_t off = 0;
+        for (uint32_t k = cls + 1; k < 32; ++k) off += ctl->big_class[k];
+        d.bigs[off + atomicAdd(&ctl->big_fill[cls], 1u)] = t;
+    }
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < C; k += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t t = d.ioff[k] + d.iflag[k] - 1u;
         const uint32_t s = d.istart[t], e = d.istart[t + 1];
@@ -275,7 +288,7 @@ __device__ __forceinline__ void island_solve_shared(const StepArgs& a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     extern __shared__ uint32_t s_cnt[];   // a.local_cap byte counters
-    __shared__ uint32_t s_head, s_tail, s_done;
+    __shared__ uint32_t s_head, s_tail, s_done, s_bi;
     __shared__ int s_fail;
     const DevWorld& d = a.d;
     double* wout = a.warm ? d.wimp[ctl->wsel ^ 1] : nullptr;
@@ -284,9 +297,16 @@ __device__ __forceinline__ void island_solve_shared(const StepArgs& a) {
     const uint32_t lt = (1u << lane) - 1u;
     constexpr uint32_t kNone = 0xfffffffeu;
     using BlockAtomic = cuda::atomic_ref<uint32_t, cuda::thread_scope_block>;
-    for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
-        if (*(volatile uint32_t*)&ctl->solve_timeout) break;   // a wait ran out: stop, the step is an error
-        const uint32_t t = d.big[bi];
+    while (true) {
+        // Thread 0 claims the next island (largest size classes first) and
+        // reads the failure flag; the block acts on both together.
+        __syncthreads();   // every thread has read the previous claim
+        if (threadIdx.x == 0)
+            s_bi = *(volatile uint32_t*)&ctl->solve_timeout ? nbig : atomicAdd(&ctl->big_next, 1u);
+        __syncthreads();
+        const uint32_t bi = s_bi;
+        if (bi >= nbig) break;   // no island left, or a wait ran out elsewhere (the step is an error)
+        const uint32_t t = d.bigs[bi];
         const uint32_t s = d.istart[t], e = d.istart[t + 1];
         const uint32_t m = e - s;
         if (m > a.local_cap) continue;

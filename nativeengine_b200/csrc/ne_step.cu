@@ -230,6 +230,8 @@ __global__ void k_step_begin(Ctl* ctl, int sticky) {
     ctl->max_island = 0;
     ctl->epa_cap_hits = 0;
     ctl->nbig = 0;
+    for (int k = 0; k < 32; ++k) ctl->big_class[k] = ctl->big_fill[k] = 0;
+    ctl->big_next = 0;
     ctl->solve_timeout = 0;
     ctl->S_stage = 0;
 }
@@ -1256,6 +1258,7 @@ struct ItemsF64 {
         }
         if (wimp_out) wimp_out[c] = solve::ld_state<C>(d.con_imp + c).x;
     }
+
 };
 
 __global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
