@@ -100,7 +100,7 @@ CONFIGS = {
 ADJ_STEPS, ADJ_K = 120, 10
 # Reference-CPU sample per config: physics steps timed on one host core.
 CPU_SAMPLE_STEPS = {"box_pile": 3, "box_pile_8": 20, "gas": 2000, "granular": 2, "batch": 2, "batch_256": 2}
-PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "solve_box_pile_512.md")
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "solve_shared_box_pile_512.md")
 
 
 def parse_args():
