@@ -18,8 +18,9 @@
  *  - Vectors are interleaved: x[3*i+0..2]; quaternions are (w,x,y,z) like ne::Q
  *    (src/vmath.hpp:47-48).
  *  - Features that the reference supports but this device path does not yet run
- *    (joints, sleeping, CCD, triangle meshes, compounds) make ne_world_upload /
- *    ne_world_step return NE_ERR_UNSUPPORTED.  There is no CPU fallback.
+ *    (joints, sleeping, CCD; triangle meshes and compounds in the FP32 form)
+ *    make ne_world_upload / ne_world_step return NE_ERR_UNSUPPORTED.  There is
+ *    no CPU fallback.
  */
 #ifndef NE_CUDA_H
 #define NE_CUDA_H
@@ -97,6 +98,25 @@ typedef struct NeWorldParams {
 /* Fills p with ne::World's defaults (src/world.hpp:75-126, src/box.hpp:17-18). */
 void ne_world_params_default(NeWorldParams* p);
 
+/* A static triangle mesh with its AABB BVH, exactly as ne::MeshData holds it
+ * after MeshData::build() (src/mesh.hpp:14-26): the device walks the given
+ * nodes in the reference's order (src/mesh.hpp:44-57), so pass the arrays of
+ * the reference's own build for contacts in the reference's order. */
+typedef struct NeMeshData {
+    uint32_t n_verts;
+    const double* verts;        /* [3*n_verts] mesh-frame vertices               */
+    uint32_t n_tris;
+    const int32_t* tris;        /* [3*n_tris] vertex indices a, b, c             */
+    const int32_t* order;       /* [n_tris] BVH-sorted triangle indices          */
+    uint32_t n_nodes;
+    const double* node_lo;      /* [3*n_nodes] node AABB                         */
+    const double* node_hi;      /* [3*n_nodes]                                   */
+    const int32_t* node_left;   /* [n_nodes] child node indices (-1: leaf)       */
+    const int32_t* node_right;  /* [n_nodes]                                     */
+    const int32_t* node_start;  /* [n_nodes] leaf range [start, start+count) of order */
+    const int32_t* node_count;  /* [n_nodes]                                     */
+} NeMeshData;
+
 /* Host-side body arrays (structure of arrays, n bodies).  Mirrors the fields of
  * ne::Body (src/body.hpp:41-130) that step() reads or writes.  For upload every
  * pointer except verts/nocollide (when unused) must be non-NULL; for download
@@ -136,6 +156,23 @@ typedef struct NeBodyArrays {
     uint32_t* nocollide_count;  /* [n]                                       */
     uint32_t* nocollide;    /* [n_nocollide] excluded partner indices         */
     uint32_t n_nocollide;
+    /* compound bodies (NE_SHAPE_COMPOUND): children as ne::ChildShape
+     * (src/body.hpp:28-39), primitives only (sphere, box, cylinder, capsule);
+     * NULL when no body is a compound */
+    uint32_t* child_offset; /* [n] first child of each compound body          */
+    uint32_t* child_count;  /* [n]                                           */
+    uint32_t n_children;
+    int32_t* child_shape;   /* [n_children] NE_SHAPE_*                       */
+    double* child_pos;      /* [3*n_children] localPos                       */
+    double* child_rot;      /* [4*n_children] localRot (w,x,y,z)             */
+    double* child_radius;   /* [n_children]                                  */
+    double* child_half_height; /* [n_children]                               */
+    double* child_half_extents; /* [3*n_children]                            */
+    /* triangle-mesh bodies (NE_SHAPE_MESH): mesh_index[i] into meshes; NULL
+     * when no body is a mesh */
+    uint32_t* mesh_index;   /* [n]                                           */
+    uint32_t n_meshes;
+    const NeMeshData* meshes; /* [n_meshes]                                  */
 } NeBodyArrays;
 
 /* One resolved contact constraint of the last step, in solver order

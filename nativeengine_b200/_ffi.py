@@ -66,6 +66,18 @@ class NeWorldParams(C.Structure):
     ]
 
 
+_i32cp = C.POINTER(C.c_int32)
+
+
+class NeMeshData(C.Structure):
+    _fields_ = [
+        ("n_verts", C.c_uint32), ("verts", C.POINTER(C.c_double)),
+        ("n_tris", C.c_uint32), ("tris", _i32cp), ("order", _i32cp),
+        ("n_nodes", C.c_uint32), ("node_lo", C.POINTER(C.c_double)), ("node_hi", C.POINTER(C.c_double)),
+        ("node_left", _i32cp), ("node_right", _i32cp), ("node_start", _i32cp), ("node_count", _i32cp),
+    ]
+
+
 class NeBodyArrays(C.Structure):
     _fields_ = [
         ("n", C.c_uint32),
@@ -78,6 +90,10 @@ class NeBodyArrays(C.Structure):
         ("layer", _u32p), ("mask", _u32p), ("flags", _u32p),
         ("nocollide_offset", _u32p), ("nocollide_count", _u32p), ("nocollide", _u32p),
         ("n_nocollide", C.c_uint32),
+        ("child_offset", _u32p), ("child_count", _u32p), ("n_children", C.c_uint32),
+        ("child_shape", _i32p), ("child_pos", _dp), ("child_rot", _dp), ("child_radius", _dp),
+        ("child_half_height", _dp), ("child_half_extents", _dp),
+        ("mesh_index", _u32p), ("n_meshes", C.c_uint32), ("meshes", C.POINTER(NeMeshData)),
     ]
 
 

@@ -87,6 +87,111 @@ def convex_mass(verts, density):
     return _inv(m), (_inv(Ix), _inv(Iy), _inv(Iz))
 
 
+class MeshData:
+    """A static triangle mesh and its AABB BVH in the layout of ne::MeshData
+    (src/mesh.hpp:14-26): vertices, triangles, BVH-sorted triangle order and
+    nodes (lo, hi, left, right, start, count; leaves of at most 4 triangles).
+
+    ``build()`` makes a BVH of its own (median split of the centroids along the
+    longest axis, stable order); any valid BVH gives the same set of contacts,
+    and the order of a mesh pair's contacts follows the BVH walk.  For contacts
+    in the reference's order, pass the arrays of the reference's own
+    MeshData::build() via ``from_arrays``."""
+
+    def __init__(self, verts, tris):
+        self.verts = np.ascontiguousarray(np.asarray(verts, dtype=np.float64).reshape(-1, 3))
+        self.tris = np.ascontiguousarray(np.asarray(tris, dtype=np.int32).reshape(-1, 3))
+        self.order = np.zeros(0, np.int32)
+        self.node_lo = self.node_hi = np.zeros((0, 3))
+        self.node_left = self.node_right = self.node_start = self.node_count = np.zeros(0, np.int32)
+
+    @classmethod
+    def from_arrays(cls, verts, tris, order, node_lo, node_hi, node_left, node_right, node_start, node_count):
+        m = cls(verts, tris)
+        m.order = np.ascontiguousarray(order, dtype=np.int32)
+        m.node_lo = np.ascontiguousarray(np.asarray(node_lo, np.float64).reshape(-1, 3))
+        m.node_hi = np.ascontiguousarray(np.asarray(node_hi, np.float64).reshape(-1, 3))
+        m.node_left, m.node_right, m.node_start, m.node_count = (
+            np.ascontiguousarray(a, dtype=np.int32) for a in (node_left, node_right, node_start, node_count))
+        return m
+
+    def build(self) -> "MeshData":
+        tv = self.verts[self.tris]                       # [m, 3, 3]
+        lo_t, hi_t = tv.min(axis=1), tv.max(axis=1)
+        cen = lo_t + hi_t
+        order = list(range(len(self.tris)))
+        lo_l, hi_l, left, right, start, count = [], [], [], [], [], []
+
+        def node(s, c):
+            idx = len(lo_l)
+            ids = order[s:s + c]
+            lo, hi = lo_t[ids].min(axis=0), hi_t[ids].max(axis=0)
+            lo_l.append(lo); hi_l.append(hi)
+            left.append(-1); right.append(-1); start.append(0); count.append(0)
+            if c <= 4:
+                start[idx], count[idx] = s, c
+                return idx
+            ext = hi - lo
+            axis = 0 if (ext[0] > ext[1] and ext[0] > ext[2]) else (1 if ext[1] > ext[2] else 2)
+            order[s:s + c] = sorted(ids, key=lambda t: cen[t, axis])
+            mid = c // 2
+            left[idx] = node(s, mid)
+            right[idx] = node(s + mid, c - mid)
+            return idx
+        if len(self.tris):
+            node(0, len(self.tris))
+        self.order = np.array(order, dtype=np.int32)
+        self.node_lo = np.array(lo_l, dtype=np.float64).reshape(-1, 3)
+        self.node_hi = np.array(hi_l, dtype=np.float64).reshape(-1, 3)
+        self.node_left, self.node_right, self.node_start, self.node_count = (
+            np.array(a, dtype=np.int32) for a in (left, right, start, count))
+        return self
+
+    def c(self) -> _ffi.NeMeshData:
+        def dp(a):
+            return a.ctypes.data_as(C.POINTER(C.c_double))
+
+        def ip(a):
+            return a.ctypes.data_as(C.POINTER(C.c_int32))
+        m = _ffi.NeMeshData()
+        m.n_verts, m.verts = len(self.verts), dp(self.verts)
+        m.n_tris, m.tris, m.order = len(self.tris), ip(self.tris), ip(self.order)
+        m.n_nodes = len(self.node_left)
+        m.node_lo, m.node_hi = dp(self.node_lo), dp(self.node_hi)
+        m.node_left, m.node_right = ip(self.node_left), ip(self.node_right)
+        m.node_start, m.node_count = ip(self.node_start), ip(self.node_count)
+        return m
+
+
+@dataclass
+class Child:
+    """ne::ChildShape (src/body.hpp:28-39): a primitive at a local transform."""
+    shape: int
+    pos: tuple = (0.0, 0.0, 0.0)
+    rot: tuple = (1.0, 0.0, 0.0, 0.0)
+    radius: float = 1.0
+    half_height: float = 0.0
+    half_extents: tuple = (0.0, 0.0, 0.0)
+
+
+def child_sphere(pos, r) -> Child:
+    return Child(_ffi.SPHERE, pos=tuple(map(float, pos)), radius=float(r))
+
+
+def child_box(pos, q, he) -> Child:
+    return Child(_ffi.BOX, pos=tuple(map(float, pos)), rot=tuple(map(float, q)), half_extents=tuple(map(float, he)))
+
+
+def child_cylinder(pos, q, r, hh) -> Child:
+    return Child(_ffi.CYLINDER, pos=tuple(map(float, pos)), rot=tuple(map(float, q)), radius=float(r),
+                 half_height=float(hh))
+
+
+def child_capsule(pos, q, r, hh) -> Child:
+    return Child(_ffi.CAPSULE, pos=tuple(map(float, pos)), rot=tuple(map(float, q)), radius=float(r),
+                 half_height=float(hh))
+
+
 @dataclass
 class Body:
     shape: int
@@ -111,6 +216,8 @@ class Body:
     mask: int = 0xFFFFFFFF
     flags: int = _ffi.DYNAMIC
     nocollide: List[int] = field(default_factory=list)
+    children: Optional[List[Child]] = None
+    mesh: Optional[MeshData] = None
 
 
 def make_sphere(x, radius, density) -> Body:
@@ -144,6 +251,42 @@ def make_convex(x, q, verts, density) -> Body:
 
 def make_plane(point, normal) -> Body:
     return Body(_ffi.PLANE, x=tuple(map(float, point)), half_extents=_normalized3(normal), inv_mass=0.0,
+                inv_inertia=(0.0, 0.0, 0.0), flags=0)
+
+
+def _child_mass(ch: Child, density):
+    if ch.shape == _ffi.BOX:
+        return box_mass(ch.half_extents, density)
+    if ch.shape == _ffi.CYLINDER:
+        return cylinder_mass(ch.radius, 2.0 * ch.half_height, density)
+    if ch.shape == _ffi.CAPSULE:
+        return capsule_mass(ch.radius, ch.half_height, density)
+    return sphere_mass(ch.radius, density)
+
+
+def make_compound(x, q, children: Sequence[Child], density) -> Body:
+    """makeCompound (src/body.hpp:372-400): mass sums the children; the inertia
+    is the diagonal of the summed tensor by the parallel-axis theorem."""
+    M = 0.0
+    Ix = Iy = Iz = 0.0
+    for ch in children:
+        im, ii = _child_mass(ch, density)
+        mc = 1.0 / im if im > 0 else 0.0
+        icx = 1.0 / ii[0] if ii[0] > 0 else 0.0
+        icy = 1.0 / ii[1] if ii[1] > 0 else 0.0
+        icz = 1.0 / ii[2] if ii[2] > 0 else 0.0
+        ox, oy, oz = ch.pos
+        M += mc
+        Ix += icx + mc * (oy * oy + oz * oz)
+        Iy += icy + mc * (ox * ox + oz * oz)
+        Iz += icz + mc * (ox * ox + oy * oy)
+    return Body(_ffi.COMPOUND, x=tuple(map(float, x)), q=tuple(map(float, q)), children=list(children),
+                inv_mass=_inv(M), inv_inertia=(_inv(Ix), _inv(Iy), _inv(Iz)))
+
+
+def make_mesh(x, q, mesh: MeshData) -> Body:
+    """makeMesh (src/body.hpp:319-331): static, placed by (x, q)."""
+    return Body(_ffi.MESH, x=tuple(map(float, x)), q=tuple(map(float, q)), mesh=mesh, inv_mass=0.0,
                 inv_inertia=(0.0, 0.0, 0.0), flags=0)
 
 
@@ -215,12 +358,37 @@ class BodyArrays:
         self.nocollide_count = np.array(nc, dtype=np.uint32)
         self.nocollide = np.array(nl if nl else [0], dtype=np.uint32)
         self.n_nocollide = len(nl)
+        co, cc, cl = [], [], []
+        for b in bodies:
+            co.append(len(cl))
+            ch = b.children or []
+            cc.append(len(ch))
+            cl.extend(ch)
+        self.child_offset = np.array(co, dtype=np.uint32)
+        self.child_count = np.array(cc, dtype=np.uint32)
+        self.n_children = len(cl)
+        cl = cl or [Child(_ffi.SPHERE)]
+        self.child_shape = np.array([c.shape for c in cl], dtype=np.int32)
+        self.child_pos = np.array([c.pos for c in cl], dtype=f64).reshape(-1, 3)
+        self.child_rot = np.array([c.rot for c in cl], dtype=f64).reshape(-1, 4)
+        self.child_radius = np.array([c.radius for c in cl], dtype=f64)
+        self.child_half_height = np.array([c.half_height for c in cl], dtype=f64)
+        self.child_half_extents = np.array([c.half_extents for c in cl], dtype=f64).reshape(-1, 3)
+        self.meshes = []
+        mi = []
+        for b in bodies:
+            if b.mesh is not None:
+                mi.append(len(self.meshes))
+                self.meshes.append(b.mesh)
+            else:
+                mi.append(0)
+        self.mesh_index = np.array(mi, dtype=np.uint32)
         self._c = None
 
     def copy(self) -> "BodyArrays":
         other = BodyArrays.__new__(BodyArrays)
         for k, v in self.__dict__.items():
-            other.__dict__[k] = v.copy() if isinstance(v, np.ndarray) else v
+            other.__dict__[k] = v.copy() if isinstance(v, np.ndarray) else (list(v) if isinstance(v, list) else v)
         other._c = None
         return other
 
@@ -257,6 +425,18 @@ class BodyArrays:
         s.nocollide_offset, s.nocollide_count, s.nocollide = (
             up(self.nocollide_offset), up(self.nocollide_count), up(self.nocollide))
         s.n_nocollide = self.n_nocollide
+        if getattr(self, "n_children", 0):
+            s.child_offset, s.child_count = up(self.child_offset), up(self.child_count)
+            s.n_children = self.n_children
+            s.child_shape = self.child_shape.ctypes.data_as(C.POINTER(C.c_int32))
+            s.child_pos, s.child_rot = dp(self.child_pos), dp(self.child_rot)
+            s.child_radius, s.child_half_height = dp(self.child_radius), dp(self.child_half_height)
+            s.child_half_extents = dp(self.child_half_extents)
+        if getattr(self, "meshes", None):
+            self._mesh_c = (_ffi.NeMeshData * len(self.meshes))(*[m.c() for m in self.meshes])
+            s.mesh_index = up(self.mesh_index)
+            s.n_meshes = len(self.meshes)
+            s.meshes = self._mesh_c
         self._c = s
         return s
 
@@ -298,6 +478,18 @@ def params_dict(p: _ffi.NeWorldParams) -> dict:
     return d
 
 
+def _set_child_arrays(out, ranges, total):
+    """Child-shape arrays of `out` from child rows [c0, c1) of each source."""
+    names = ("child_shape", "child_pos", "child_rot", "child_radius", "child_half_height", "child_half_extents")
+    out.n_children = total
+    for k in names:
+        rows = [getattr(b, k)[c0:c1] for b, c0, c1 in ranges]
+        if total:
+            setattr(out, k, np.ascontiguousarray(np.concatenate(rows)))
+        else:
+            setattr(out, k, np.ascontiguousarray(getattr(ranges[0][0], k)[:1]) if ranges else None)
+
+
 def concat(parts):
     """Concatenate BodyArrays into one batch; returns (BodyArrays, world_begin).
     Convex vertex offsets and noCollide indices are rebased onto the batch."""
@@ -328,6 +520,19 @@ def concat(parts):
     out.n_nocollide = nbase
     nc = np.concatenate(ncl) if nbase else np.zeros(1)
     out.nocollide = np.ascontiguousarray(nc, dtype=np.uint32)
+    co, cparts, mi, meshes = [], [], [], []
+    cbase = 0
+    for b in parts:
+        co.append(b.child_offset.astype(np.int64) + cbase)
+        cparts.append(b)
+        cbase += b.n_children
+        mi.append(b.mesh_index.astype(np.int64) + len(meshes))
+        meshes.extend(b.meshes)
+    out.child_offset = np.concatenate(co).astype(np.uint32)
+    out.child_count = np.ascontiguousarray(np.concatenate([b.child_count for b in parts]))
+    _set_child_arrays(out, [(b, 0, b.n_children) for b in parts], cbase)
+    out.mesh_index = np.concatenate(mi).astype(np.uint32)
+    out.meshes = meshes
     out._c = None
     return out, np.array(begin, dtype=np.uint32)
 
@@ -367,5 +572,12 @@ def take_range(bodies: BodyArrays, b0: int, b1: int) -> BodyArrays:
     out.nocollide_offset = np.array(no, dtype=np.uint32)
     out.n_nocollide = nbase
     out.nocollide = np.ascontiguousarray(np.concatenate(ncl) if nbase else np.zeros(1), dtype=np.uint32)
+    c0 = int(bodies.child_offset[b0]) if b1 > b0 else 0
+    c1 = int(bodies.child_offset[b1 - 1] + bodies.child_count[b1 - 1]) if b1 > b0 else 0
+    out.child_offset = (bodies.child_offset[b0:b1].astype(np.int64) - c0).astype(np.uint32)
+    out.child_count = np.ascontiguousarray(bodies.child_count[b0:b1])
+    _set_child_arrays(out, [(bodies, c0, c1)], c1 - c0)
+    out.mesh_index = np.ascontiguousarray(bodies.mesh_index[b0:b1])
+    out.meshes = list(bodies.meshes)
     out._c = None
     return out

@@ -9,6 +9,7 @@
 // runs the step again -- so growth never changes the result, and steady-state
 // steps cost one small device->host read of the control block.
 #include <algorithm>
+#include <type_traits>
 #include <thread>
 #include <cmath>
 #include <cstdio>
@@ -86,6 +87,7 @@ struct NeWorld {
     uint32_t big_ctas_per_sm = 1;
     uint32_t big_team_max = 1;
     bool shape_chosen = false;            // set by the caller or the autotuner (else per upload)
+    bool has_ext = false;                 // some body is a triangle mesh or a compound
     size_t nverts = 0;                    // convex vertex pool entries on the device
     uint64_t Rcap = 0;                    // capacity of the recorded pair list
     int key_bits = 64;
@@ -179,6 +181,7 @@ void free_con_arrays(NeWorld* w) {
     dfree(d.ioff); dfree(d.istart); dfree(d.big); dfree(d.con_kn);
     dfree(d.rkey[0]); dfree(d.rkey[1]); dfree(d.rval[0]); dfree(d.rval[1]); dfree(d.crank);
     dfree(d.bcnt10); dfree(d.bq10); dfree(d.bctl); dfree(d.bteam); dfree(d.brec); dfree(d.bigs);
+    dfree(d.ext_cn); dfree(d.ext_cp);
     free_f32_cons(w);
 }
 
@@ -224,7 +227,8 @@ int alloc_cons(NeWorld* w, uint64_t cap) {
         (rc = dalloc(&d.rval[1], 2 * cap)) || (rc = dalloc(&d.crank, 2 * cap)) ||
         (rc = dalloc(&d.bcnt10, 10 * cap)) || (rc = dalloc(&d.bq10, 10 * cap)) ||
         (rc = dalloc(&d.bctl, cap / neb::kBigIsland + 1)) || (rc = dalloc(&d.bteam, cap / neb::kBigIsland + 2)) ||
-        (rc = dalloc(&d.brec, 2 * cap)) || (rc = dalloc(&d.bigs, cap / neb::kBigIsland + 1)))
+        (rc = dalloc(&d.brec, 2 * cap)) || (rc = dalloc(&d.bigs, cap / neb::kBigIsland + 1)) ||
+        (rc = dalloc(&d.ext_cn, cap)) || (rc = dalloc(&d.ext_cp, cap)))
         return rc;
     if (w->precision == NE_PRECISION_F32 && (rc = alloc_f32_cons(w, cap))) return rc;
     unsigned long long* nk[2] = {nullptr, nullptr};
@@ -275,6 +279,7 @@ neb::StepArgs make_args(const NeWorld* w) {
     a.Rcap = w->Rcap;
     a.num_sms = w->num_sms;
     a.local_cap = neb::kLocalCap;
+    a.any_ext = w->has_ext ? 1 : 0;
     return a;
 }
 
@@ -477,6 +482,8 @@ int ne_world_destroy(NeWorld* w) {
     free_con_arrays(w);
     neb::DevWorld& d = w->d;
     dfree(d.verts); dfree(d.nc); dfree(d.planes); dfree(d.io);
+    dfree(d.child); dfree(d.mesh_tab); dfree(d.mnode_lo); dfree(d.mnode_hi); dfree(d.mnode); dfree(d.morder);
+    dfree(d.mtri); dfree(d.mvert);
     for (int b = 0; b < 2; ++b) { dfree(d.wkey[b]); dfree(d.wimp[b]); }
     dfree(d.hist); dfree(d.tsum); dfree(d.ctl);
     dfree(w->d_wp); dfree(w->d_bw); dfree(w->d_cext); dfree(d.xlist); dfree(d.rec_i); dfree(d.rec_j);
@@ -510,6 +517,107 @@ int ne_world_set_params(NeWorld* w, const NeWorldParams* params) {
 
 namespace {
 
+// Every index a BVH walk or a triangle reads stays inside its arrays.
+int check_mesh(const NeMeshData& m) {
+    if (m.n_tris && (!m.verts || !m.tris || !m.order)) return set_err(NE_ERR_ARG, "mesh arrays are NULL");
+    if (m.n_nodes && (!m.node_lo || !m.node_hi || !m.node_left || !m.node_right || !m.node_start || !m.node_count))
+        return set_err(NE_ERR_ARG, "mesh BVH arrays are NULL");
+    for (uint32_t t = 0; t < 3 * m.n_tris; ++t)
+        if (m.tris[t] < 0 || (uint32_t)m.tris[t] >= m.n_verts) return set_err(NE_ERR_ARG, "mesh vertex index out of range");
+    for (uint32_t t = 0; t < m.n_tris; ++t)
+        if (m.order[t] < 0 || (uint32_t)m.order[t] >= m.n_tris) return set_err(NE_ERR_ARG, "mesh triangle order out of range");
+    for (uint32_t k = 0; k < m.n_nodes; ++k) {
+        const int l = m.node_left[k], r = m.node_right[k];
+        if (l < 0) {
+            if (m.node_start[k] < 0 || m.node_count[k] < 0 ||
+                (uint64_t)m.node_start[k] + (uint64_t)m.node_count[k] > m.n_tris)
+                return set_err(NE_ERR_ARG, "mesh BVH leaf range out of bounds");
+        } else if ((uint32_t)l >= m.n_nodes || r < 0 || (uint32_t)r >= m.n_nodes) {
+            return set_err(NE_ERR_ARG, "mesh BVH child index out of range");
+        }
+    }
+    return NE_OK;
+}
+
+// Compound children and meshes on the device.  Children: four records each,
+// (localPos, shape), localRot (w,x,y,z), (radius, halfHeight, he.x, he.y),
+// (he.z, 0, 0, 0).  Meshes: one table row per mesh (node, order, triangle and
+// vertex offsets) over concatenated node, order, triangle and vertex arrays.
+int upload_children_meshes(NeWorld* w, const NeBodyArrays* b) {
+    neb::DevWorld& d = w->d;
+    int rc;
+    const uint32_t nc = b->child_shape ? b->n_children : 0;
+    std::vector<neb::D4> ch(4 * (size_t)(nc ? nc : 1), neb::D4{0, 0, 0, 0});
+    for (uint32_t k = 0; k < nc; ++k) {
+        const double* lp = b->child_pos + 3 * (size_t)k;
+        const double* lr = b->child_rot + 4 * (size_t)k;
+        const double* he = b->child_half_extents + 3 * (size_t)k;
+        ch[4 * k + 0] = neb::D4{lp[0], lp[1], lp[2], (double)b->child_shape[k]};
+        ch[4 * k + 1] = neb::D4{lr[0], lr[1], lr[2], lr[3]};
+        ch[4 * k + 2] = neb::D4{b->child_radius[k], b->child_half_height[k], he[0], he[1]};
+        ch[4 * k + 3] = neb::D4{he[2], 0.0, 0.0, 0.0};
+    }
+    dfree(d.child);
+    if ((rc = dalloc(&d.child, ch.size()))) return rc;
+    NE_CUDA_TRY(cudaMemcpy(d.child, ch.data(), ch.size() * sizeof(neb::D4), cudaMemcpyHostToDevice));
+
+    const uint32_t nm = b->meshes ? b->n_meshes : 0;
+    std::vector<uint4> tab(nm ? nm : 1, make_uint4(0, 0, 0, 0));
+    std::vector<neb::D4> lo, hi, vs;
+    std::vector<int4> nodes, tris;
+    std::vector<int> order;
+    for (uint32_t k = 0; k < nm; ++k) {
+        const NeMeshData& m = b->meshes[k];
+        if ((rc = check_mesh(m))) return rc;
+        tab[k] = make_uint4((uint32_t)nodes.size(), (uint32_t)order.size(), (uint32_t)tris.size(), (uint32_t)vs.size());
+        for (uint32_t t = 0; t < m.n_nodes; ++t) {
+            lo.push_back(neb::D4{m.node_lo[3 * t], m.node_lo[3 * t + 1], m.node_lo[3 * t + 2], 0.0});
+            hi.push_back(neb::D4{m.node_hi[3 * t], m.node_hi[3 * t + 1], m.node_hi[3 * t + 2], 0.0});
+            nodes.push_back(make_int4(m.node_left[t], m.node_right[t], m.node_start[t], m.node_count[t]));
+        }
+        for (uint32_t t = 0; t < m.n_tris; ++t) {
+            order.push_back(m.order[t]);
+            tris.push_back(make_int4(m.tris[3 * t], m.tris[3 * t + 1], m.tris[3 * t + 2], 0));
+        }
+        for (uint32_t v = 0; v < m.n_verts; ++v)
+            vs.push_back(neb::D4{m.verts[3 * v], m.verts[3 * v + 1], m.verts[3 * v + 2], 0.0});
+        if (!m.n_nodes) tab[k].x = 0xffffffffu;   // empty mesh: no walk
+    }
+    auto put = [&](auto*& dst, const auto& src) -> int {
+        using T = typename std::decay_t<decltype(src)>::value_type;
+        dfree(dst);
+        const size_t cnt = src.empty() ? 1 : src.size();
+        int r = dalloc(&dst, cnt);
+        if (r) return r;
+        if (!src.empty()) {
+            cudaError_t e = cudaMemcpy(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) return set_err(NE_ERR_CUDA, cudaGetErrorString(e));
+        }
+        return NE_OK;
+    };
+    if ((rc = put(d.mesh_tab, tab)) || (rc = put(d.mnode_lo, lo)) || (rc = put(d.mnode_hi, hi)) ||
+        (rc = put(d.mnode, nodes)) || (rc = put(d.morder, order)) || (rc = put(d.mtri, tris)) ||
+        (rc = put(d.mvert, vs)))
+        return rc;
+    return NE_OK;
+}
+
+// Bounding radius of a compound (src/body.hpp:147-155).
+double compound_bound(const NeBodyArrays* b, uint32_t i) {
+    double m = 0.0;
+    for (uint32_t k = b->child_offset[i]; k < b->child_offset[i] + b->child_count[i]; ++k) {
+        const int cs = b->child_shape[k];
+        const double* he = b->child_half_extents + 3 * (size_t)k;
+        const double* lp = b->child_pos + 3 * (size_t)k;
+        const double cr = (cs == NE_SHAPE_SPHERE) ? b->child_radius[k]
+                        : (cs == NE_SHAPE_BOX) ? std::sqrt(he[0] * he[0] + he[1] * he[1] + he[2] * he[2])
+                                               : b->child_half_height[k] + b->child_radius[k];
+        const double r = std::sqrt(lp[0] * lp[0] + lp[1] * lp[1] + lp[2] * lp[2]) + cr;
+        m = std::max(m, r);
+    }
+    return m;
+}
+
 int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const uint32_t* wbegin,
                 const NeBodyArrays* b) {
     const uint32_t n = b->n;
@@ -530,8 +638,24 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
     for (uint32_t i = 0; i < n; ++i) {
         const int s = b->shape[i];
         if (s < 0 || s > NE_SHAPE_COMPOUND) return set_err(NE_ERR_ARG, "shape tag out of range");
-        if (s == NE_SHAPE_MESH || s == NE_SHAPE_COMPOUND)
-            return set_err(NE_ERR_UNSUPPORTED, "triangle meshes and compounds are not on the device path");
+        if ((s == NE_SHAPE_MESH || s == NE_SHAPE_COMPOUND) && w->precision == NE_PRECISION_F32)
+            return set_err(NE_ERR_UNSUPPORTED, "triangle meshes and compounds are not in the FP32 form");
+        if (s == NE_SHAPE_COMPOUND) {
+            if (!b->child_offset || !b->child_count || !b->child_shape || !b->child_pos || !b->child_rot ||
+                !b->child_radius || !b->child_half_height || !b->child_half_extents)
+                return set_err(NE_ERR_ARG, "compound body without child arrays");
+            if ((uint64_t)b->child_offset[i] + b->child_count[i] > b->n_children)
+                return set_err(NE_ERR_ARG, "compound child range out of bounds");
+            for (uint32_t k = b->child_offset[i]; k < b->child_offset[i] + b->child_count[i]; ++k) {
+                const int cs = b->child_shape[k];
+                if (cs != NE_SHAPE_SPHERE && cs != NE_SHAPE_BOX && cs != NE_SHAPE_CYLINDER && cs != NE_SHAPE_CAPSULE)
+                    return set_err(NE_ERR_ARG, "compound children are spheres, boxes, cylinders or capsules");
+            }
+        }
+        if (s == NE_SHAPE_MESH) {
+            if (!b->mesh_index || !b->meshes || b->mesh_index[i] >= b->n_meshes)
+                return set_err(NE_ERR_ARG, "mesh body without a valid mesh");
+        }
         if (s == NE_SHAPE_CONVEX) {
             if (!b->verts || !b->vert_offset || !b->vert_count) return set_err(NE_ERR_ARG, "convex body without vertices");
             if ((uint64_t)b->vert_offset[i] + b->vert_count[i] > b->n_verts)
@@ -602,6 +726,10 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
     NE_CUDA_TRY(cudaMemcpy(d.verts, verts.data(), verts.size() * sizeof(neb::D4), cudaMemcpyHostToDevice));
     w->nverts = b->n_verts;
     if (w->precision == NE_PRECISION_F32 && (rc = alloc_f32_bodies(w))) return rc;
+    if ((rc = upload_children_meshes(w, b))) return rc;
+    w->has_ext = false;
+    for (uint32_t i = 0; i < n; ++i)
+        if (b->shape[i] == NE_SHAPE_MESH || b->shape[i] == NE_SHAPE_COMPOUND) w->has_ext = true;
 
     std::vector<double> boundR(n);
     std::vector<int> shapes(n);
@@ -612,7 +740,8 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
         const neb::V3 he = neb::mk(b->half_extents[3 * i], b->half_extents[3 * i + 1], b->half_extents[3 * i + 2]);
         const neb::D4* vp = (s == NE_SHAPE_CONVEX) ? verts.data() + b->vert_offset[i] : verts.data();
         const int nv = (s == NE_SHAPE_CONVEX) ? (int)b->vert_count[i] : 0;
-        boundR[i] = neb::bounding_radius(s, b->radius[i], b->half_height[i], he, vp, nv);
+        boundR[i] = (s == NE_SHAPE_COMPOUND) ? compound_bound(b, i)
+                                             : neb::bounding_radius(s, b->radius[i], b->half_height[i], he, vp, nv);
         if (s == NE_SHAPE_PLANE || s == NE_SHAPE_MESH) planes.push_back(i);
         st[i] = v3(b->inv_inertia, i, boundR[i]);
     }
@@ -651,7 +780,10 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
         if (mut) fl |= neb::kFlagMutable;
         if (w->h_large[i]) fl |= neb::kFlagLarge;
         meta[i] = make_uint4((uint32_t)b->shape[i], fl, b->layer[i], b->mask[i]);
-        vr[i] = (b->shape[i] == NE_SHAPE_CONVEX) ? make_uint2(b->vert_offset[i], b->vert_count[i]) : make_uint2(0, 0);
+        vr[i] = (b->shape[i] == NE_SHAPE_CONVEX)     ? make_uint2(b->vert_offset[i], b->vert_count[i])
+                : (b->shape[i] == NE_SHAPE_COMPOUND) ? make_uint2(b->child_offset[i], b->child_count[i])
+                : (b->shape[i] == NE_SHAPE_MESH)     ? make_uint2(b->mesh_index[i], 0)
+                                                     : make_uint2(0, 0);
         ncr[i] = (b->nocollide_count && b->nocollide_count[i])
                      ? make_uint2(b->nocollide_offset[i], b->nocollide_count[i])
                      : make_uint2(0, 0);
@@ -1081,6 +1213,8 @@ int ne_world_set_precision(NeWorld* w, int precision) {
     NE_CUDA_TRY(cudaSetDevice(w->device));
     NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
     if (precision == w->precision) return NE_OK;
+    if (precision == NE_PRECISION_F32 && w->has_ext)
+        return set_err(NE_ERR_UNSUPPORTED, "triangle meshes and compounds are not in the FP32 form");
     w->precision = precision;
     int rc;
     if (precision == NE_PRECISION_F32) {

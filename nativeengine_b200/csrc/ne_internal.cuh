@@ -139,6 +139,15 @@ struct DevWorld {
     uint32_t* bteam;         // [C/48 + 2] first virtual CTA of each big island's team
     uint32_t* bigs;          // [C/48 + 1] big islands, larger size classes first
     uint4* brec;             // [2C] per island position: {c, i, j, flags}, {next on i, next on j} (big islands)
+    // compound children and triangle meshes (vrng: child range; mesh index in .x)
+    D4* child;               // [4 per child] (localPos, shape), localRot, (r, hh, he.x, he.y), (he.z, -, -, -)
+    uint4* mesh_tab;         // [meshes] node, order, triangle and vertex offsets (node offset ~0u: empty)
+    D4 *mnode_lo, *mnode_hi; // [nodes] BVH node bounds
+    int4* mnode;             // [nodes] (left, right, start, count), mesh-local
+    int* morder;             // [tris] BVH-sorted triangle indices, mesh-local
+    int4* mtri;              // [tris] vertex indices, mesh-local
+    D4* mvert;               // [verts] mesh-frame vertices
+    D4 *ext_cn, *ext_cp;     // [C] contacts of mesh and compound pairs, at their constraint index
     // batched FP32 form (null in FP64 mode): FP32 copies of the body state the
     // narrowphase and the solver read, refreshed every step after integration,
     // and the FP32 constraint records.  Poses, the warm-start impulses and the

@@ -894,6 +894,164 @@ __global__ void __launch_bounds__(kT) k_surv_place(StepArgs a) {
     }
 }
 
+// ---- triangle meshes and compounds (src/world.cpp:53-121) --------------------
+// A pair with a mesh or a compound can have any number of contacts: the
+// narrowphase counts them, and once the scan has placed every pair,
+// k_narrowphase_ext computes them again and writes them at their constraint
+// index (ext_cn / ext_cp).  Both passes run the same arithmetic, so they agree.
+
+__device__ __forceinline__ bool is_ext_shape(int s) { return s == SH_MESH || s == SH_COMPOUND; }
+
+// A compound's child as a body of its own (compoundChildWorld, src/body.hpp:358-366).
+__device__ __forceinline__ BodyG child_world(const DevWorld& d, const BodyG& parent, uint32_t k) {
+    const D4 c0 = d.child[4 * k], c1 = d.child[4 * k + 1], c2 = d.child[4 * k + 2], c3 = d.child[4 * k + 3];
+    BodyG c;
+    c.x = parent.x + rotate(parent.q, mk(c0.x, c0.y, c0.z));
+    c.q = qmul(parent.q, qof(c1));
+    c.he = mk(c2.z, c2.w, c3.x);
+    c.radius = c2.x;
+    c.half_height = c2.y;
+    c.verts = nullptr;
+    c.nverts = 0;
+    c.shape = (int)c0.w;
+    return c;
+}
+
+// Sink for the contacts of one pair: counts them, and writes them (normal
+// b -> a, flipped when `flip`) when `cn` is set, up to `cap`.
+struct ExtOut {
+    D4 *cn, *cp;
+    uint32_t cap, n;
+    bool flip;
+    __device__ __forceinline__ void add(const Contact& c) {
+        if (cn && n < cap) {
+            const V3 nrm = flip ? -c.normal : c.normal;
+            cn[n] = d4of(nrm, c.overlap);
+            cp[n] = d4of(c.point, 0.0);
+        }
+        ++n;
+    }
+};
+
+// meshContacts (src/world.cpp:56-85): every triangle of the mesh whose AABB
+// meets the other body's bounding cube (BVH walk of src/mesh.hpp:44-57, in
+// its order), as a 1e-3-thick prism through the narrowphase; normals point
+// mesh -> other.
+__device__ void mesh_contacts(const DevWorld& d, const BodyG& other, double other_bound, const BodyG& mb,
+                              uint32_t mesh, const Domain& dom, EpaScratch& S, int& fl, ExtOut& out) {
+    const uint4 tab = d.mesh_tab[mesh];
+    if (tab.x == 0xffffffffu) return;
+    const V3 rel = min_image(dom, other.x - mb.x);
+    const V3 cl = inv_rotate(mb.q, rel);
+    const double rr = other_bound + 0.05;
+    const V3 lo = cl - mk(rr, rr, rr), hi = cl + mk(rr, rr, rr);
+    const double thick = 1e-3;
+    D4 pv[6];
+    BodyG tri;
+    tri.x = mk(0.0, 0.0, 0.0);
+    tri.q = mkq(1.0, 0.0, 0.0, 0.0);
+    tri.he = mk(0.0, 0.0, 0.0);
+    tri.radius = 1.0;
+    tri.half_height = 0.0;
+    tri.verts = pv;
+    tri.nverts = 6;
+    tri.shape = SH_CONVEX;
+    int stack[64];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int ni = stack[--sp];
+        const D4 nl = d.mnode_lo[tab.x + ni], nh = d.mnode_hi[tab.x + ni];
+        if (lo.x > nh.x || hi.x < nl.x || lo.y > nh.y || hi.y < nl.y || lo.z > nh.z || hi.z < nl.z) continue;
+        const int4 nd = d.mnode[tab.x + ni];
+        if (nd.x >= 0) {
+            if (sp < 62) {
+                stack[sp++] = nd.x;
+                stack[sp++] = nd.y;
+            }
+            continue;
+        }
+        for (int t = 0; t < nd.w; ++t) {
+            const int ti = d.morder[tab.y + nd.z + t];
+            const int4 tv = d.mtri[tab.z + ti];
+            const D4 a0 = d.mvert[tab.w + tv.x], a1 = d.mvert[tab.w + tv.y], a2 = d.mvert[tab.w + tv.z];
+            const V3 w0 = mb.x + rotate(mb.q, mk(a0.x, a0.y, a0.z));
+            const V3 w1 = mb.x + rotate(mb.q, mk(a1.x, a1.y, a1.z));
+            const V3 w2 = mb.x + rotate(mb.q, mk(a2.x, a2.y, a2.z));
+            V3 n = cross(w1 - w0, w2 - w0);
+            const double len = norm(n);
+            if (len < 1e-12) continue;   // degenerate triangle
+            n = n / len;
+            pv[0] = d4of(w0 + n * thick, 0.0);
+            pv[1] = d4of(w1 + n * thick, 0.0);
+            pv[2] = d4of(w2 + n * thick, 0.0);
+            pv[3] = d4of(w0 - n * thick, 0.0);
+            pv[4] = d4of(w1 - n * thick, 0.0);
+            pv[5] = d4of(w2 - n * thick, 0.0);
+            const Contact c = detect_contact(other, tri, dom, S, fl);   // normal tri -> other
+            if (c.hit) out.add(c);
+        }
+    }
+}
+
+// gatherContacts (src/world.cpp:88-121) for a pair with a mesh or a compound.
+__device__ void ext_contacts(const DevWorld& d, uint32_t i, uint32_t j, const BodyG& A, const BodyG& B,
+                             const Domain& dom, EpaScratch& S, int& fl, ExtOut& out) {
+    if (B.shape == SH_MESH) {
+        out.flip = false;
+        mesh_contacts(d, A, d.inert[i].w, B, d.vrng[j].x, dom, S, fl, out);   // mesh(b) -> a
+        return;
+    }
+    if (A.shape == SH_MESH) {
+        out.flip = true;                                                     // mesh(a) -> b, reported b -> a
+        mesh_contacts(d, B, d.inert[j].w, A, d.vrng[i].x, dom, S, fl, out);
+        return;
+    }
+    out.flip = false;
+    const uint2 ra = d.vrng[i], rb = d.vrng[j];
+    if (A.shape == SH_COMPOUND && B.shape == SH_COMPOUND) {
+        for (uint32_t ka = ra.x; ka < ra.x + ra.y; ++ka) {
+            const BodyG ba = child_world(d, A, ka);
+            for (uint32_t kb = rb.x; kb < rb.x + rb.y; ++kb) {
+                const BodyG bb = child_world(d, B, kb);
+                const Contact c = detect_contact(ba, bb, dom, S, fl);
+                if (c.hit) out.add(c);
+            }
+        }
+    } else if (A.shape == SH_COMPOUND) {
+        for (uint32_t ka = ra.x; ka < ra.x + ra.y; ++ka) {
+            const Contact c = detect_contact(child_world(d, A, ka), B, dom, S, fl);
+            if (c.hit) out.add(c);
+        }
+    } else {
+        for (uint32_t kb = rb.x; kb < rb.x + rb.y; ++kb) {
+            const Contact c = detect_contact(A, child_world(d, B, kb), dom, S, fl);
+            if (c.hit) out.add(c);
+        }
+    }
+}
+
+// Second pass over the mesh and compound pairs: their contacts at their
+// constraint index.
+__global__ void __launch_bounds__(128) k_narrowphase_ext(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    if (ctl->C > a.Ccap) return;   // k_constraint_build raises the abort
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ctl->S) return;
+    const DevWorld& d = a.d;
+    const uint32_t cnt = d.ccnt[s];
+    if (cnt == 0) return;
+    const uint32_t i = d.si[s], j = d.sj[s];
+    if (!is_ext_shape((int)d.meta[i].x) && !is_ext_shape((int)d.meta[j].x)) return;
+    const BodyG A = load_geom(d, i), B = load_geom(d, j);
+    EpaScratch S;
+    int fl = 0;
+    const uint32_t c0 = d.coff[s];
+    ExtOut out{d.ext_cn + c0, d.ext_cp + c0, cnt, 0, false};
+    ext_contacts(d, i, j, A, B, a.wp[a.bw[i]].dom, S, fl, out);
+}
+
 // gatherContacts() for one surviving pair (src/world.cpp:122-129).
 __global__ void __launch_bounds__(128) k_narrowphase(StepArgs a) {
     Ctl* ctl = a.d.ctl;
@@ -906,6 +1064,14 @@ __global__ void __launch_bounds__(128) k_narrowphase(StepArgs a) {
     EpaScratch S;
     int fl = 0;
     const Domain dom = a.wp[a.bw[i]].dom;
+    if (is_ext_shape(A.shape) || is_ext_shape(B.shape)) {
+        ExtOut out{nullptr, nullptr, 0, 0, false};
+        ext_contacts(d, i, j, A, B, dom, S, fl, out);
+        d.ccnt[s] = out.n;
+        if (fl & 1) atomicOr(&ctl->flags, 1u);
+        if (fl & 2) atomicAdd((unsigned long long*)&ctl->epa_cap_hits, 1ull);
+        return;
+    }
     Contact c = detect_contact(A, B, dom, S, fl);
     uint32_t cnt = 0;
     if (c.hit) {
@@ -1007,10 +1173,11 @@ __global__ void __launch_bounds__(kT) k_constraint_build(StepArgs a) {
     const uint32_t wn = ctl->wcount[ws];
     uint32_t widx = 0;
     if (a.warm) widx = lower_bound_u64(d.wkey[ws], 0, wn, key);
+    const bool ext = is_ext_shape((int)d.meta[i].x) || is_ext_shape((int)d.meta[j].x);
     for (uint32_t k = 0; k < cnt; ++k) {
         const uint32_t c = c0 + k;
-        const D4 cn = d.cn[4 * s + k];
-        const V3 n = v3of(cn), pt = v3of(d.cp[4 * s + k]);
+        const D4 cn = ext ? d.ext_cn[c] : d.cn[4 * s + k];
+        const V3 n = v3of(cn), pt = v3of(ext ? d.ext_cp[c] : d.cp[4 * s + k]);
         const V3 rA = min_image(W.dom, pt - xa);
         const V3 rB = min_image(W.dom, pt - xb);
         const V3 vc = (va + cross(wa, rA)) - (vb + cross(wb, rB));
@@ -1483,6 +1650,9 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
     }
     mark(4);
     scan_u32(d.ccnt, d.coff, (uint32_t)a.Scap, d.tsum, &ctl->C, ctl, st, launches, &ctl->S);
+    if (a.any_ext) {
+        k_narrowphase_ext<<<blocks_for(a.Scap, 128), 128, 0, st>>>(a); ++L;
+    }
     k_constraint_build<<<blocks_for(a.Scap, kT), kT, 0, st>>>(a); ++L;
 
     mark(5);

@@ -51,6 +51,7 @@ struct StepArgs {
     int big_team_max;        // CTAs per big island: 1 = block-local solver, > 1 = team solver (tuned)
     int sticky;              // replayed batch: an aborted step halts the rest of the batch
     uint32_t local_cap;      // big islands up to this many contacts: shared-memory dataflow solver
+    int any_ext;             // some body is a triangle mesh or a compound (second narrowphase pass)
 };
 
 // Contacts per island the shared-memory dataflow solver takes (one counter

@@ -263,6 +263,94 @@ def box_stack(levels=6, friction=0.6, dt=1.0 / 240.0):
     return params, BodyArrays(bodies)
 
 
+# ---- triangle meshes and compounds -------------------------------------------
+
+def heightfield_mesh(origin, spacing, rows, cols, heights) -> "MeshData":
+    """A rows x cols height grid (row-major heights, spacing in x/z) as a
+    triangle mesh, two triangles per cell, with its BVH."""
+    from .bodies import MeshData
+    verts = [(origin[0] + c * spacing, origin[1] + heights[r * cols + c], origin[2] + r * spacing)
+             for r in range(rows) for c in range(cols)]
+    tris = []
+    for r in range(rows - 1):
+        for c in range(cols - 1):
+            a, b, d, e = r * cols + c, r * cols + c + 1, (r + 1) * cols + c, (r + 1) * cols + c + 1
+            tris += [(a, d, b), (b, d, e)]
+    return MeshData(verts, tris).build()
+
+
+def mesh_floor(dt=1.0 / 240.0):
+    """A sphere and a box dropped on a two-triangle floor mesh (the setting of
+    the reference's mesh self-test)."""
+    from .bodies import MeshData, make_mesh
+    floor = MeshData([(-10, 0, -10), (10, 0, -10), (10, 0, 10), (-10, 0, 10)], [(0, 1, 2), (0, 2, 3)]).build()
+    bodies = [make_mesh((0.0, 0.0, 0.0), (1, 0, 0, 0), floor),
+              make_sphere((1.0, 5.0, 1.0), 0.5, 1.0),
+              make_box((-3.0, 5.0, -2.0), (1, 0, 0, 0), (0.5, 0.5, 0.5), 1.0)]
+    params = default_params(half=1000.0, dt=dt, gravity=(0.0, -10.0, 0.0), restitution=0.0, friction=0.5)
+    return params, BodyArrays(bodies)
+
+
+def terrain_drop(n=24, rows=9, cols=9, seed=12, dt=1.0 / 120.0):
+    """Spheres, boxes, capsules and hulls dropped on a bumpy height-field mesh
+    placed off the origin and turned (contacts against many triangles)."""
+    from .bodies import make_mesh
+    rng = _rng(seed)
+    h = [0.6 * math.sin(0.9 * c) * math.cos(0.7 * r) for r in range(rows) for c in range(cols)]
+    terrain = heightfield_mesh((-8.0, 0.0, -8.0), 2.0, rows, cols, h)
+    bodies = [make_mesh((0.5, -0.2, 0.3), normalized_quat((1.0, 0.0, 0.08, 0.0)), terrain)]
+    for k in range(n):
+        x = (float(rng.uniform(-5, 5)), float(2.0 + 1.3 * k), float(rng.uniform(-5, 5)))
+        kind = k % 4
+        if kind == 0:
+            bodies.append(make_sphere(x, float(rng.uniform(0.3, 0.6)), 1.0))
+        elif kind == 1:
+            bodies.append(make_box(x, random_quat(rng), tuple(rng.uniform(0.25, 0.6, 3)), 1.0))
+        elif kind == 2:
+            bodies.append(make_capsule(x, random_quat(rng), 0.3, float(rng.uniform(0.2, 0.5)), 1.0))
+        else:
+            bodies.append(make_convex(x, random_quat(rng), _hull_points(rng), 1.0))
+    params = default_params(half=1000.0, open_boundary=1, dt=dt, gravity=(0.0, -9.81, 0.0), restitution=0.2,
+                            friction=0.5)
+    return params, BodyArrays(bodies)
+
+
+def compound_pile(n=12, seed=21, dt=1.0 / 120.0, with_mesh=False):
+    """Compounds of mixed children (dumbbells, tables, capsule crosses) and
+    boxes dropped on a static floor box, or on a floor mesh: compound-box,
+    compound-compound and (with_mesh) compound-mesh contacts."""
+    from .bodies import (MeshData, child_box, child_capsule, child_cylinder, child_sphere, make_compound,
+                         make_mesh)
+    rng = _rng(seed)
+    if with_mesh:
+        floor = MeshData([(-12, 0, -12), (12, 0, -12), (12, 0, 12), (-12, 0, 12)], [(0, 1, 2), (0, 2, 3)]).build()
+        bodies = [make_mesh((0.0, 0.0, 0.0), (1, 0, 0, 0), floor)]
+    else:
+        bodies = [make_static(make_box((0.0, -1.0, 0.0), (1, 0, 0, 0), (20.0, 1.0, 20.0), 1.0))]
+    for k in range(n):
+        x = (float(rng.uniform(-3, 3)), float(2.0 + 1.6 * k), float(rng.uniform(-3, 3)))
+        q = random_quat(rng)
+        kind = k % 4
+        if kind == 0:
+            kids = [child_sphere((-0.8, 0.0, 0.0), 0.4), child_sphere((0.8, 0.0, 0.0), 0.4),
+                    child_cylinder((0.0, 0.0, 0.0), normalized_quat((1.0, 0.0, 0.0, 1.0)), 0.15, 0.6)]
+            bodies.append(make_compound(x, q, kids, 1.0))
+        elif kind == 1:
+            kids = [child_box((0.0, 0.3, 0.0), (1, 0, 0, 0), (0.8, 0.1, 0.5))] + [
+                child_box((sx * 0.6, -0.1, sz * 0.35), (1, 0, 0, 0), (0.08, 0.3, 0.08))
+                for sx in (-1, 1) for sz in (-1, 1)]
+            bodies.append(make_compound(x, q, kids, 1.0))
+        elif kind == 2:
+            kids = [child_capsule((0.0, 0.0, 0.0), (1, 0, 0, 0), 0.2, 0.6),
+                    child_capsule((0.0, 0.0, 0.0), normalized_quat((1.0, 0.0, 0.0, 1.0)), 0.2, 0.6)]
+            bodies.append(make_compound(x, q, kids, 1.0))
+        else:
+            bodies.append(make_box(x, q, tuple(rng.uniform(0.3, 0.6, 3)), 1.0))
+    params = default_params(half=1000.0, open_boundary=1, dt=dt, gravity=(0.0, -9.81, 0.0), restitution=0.1,
+                            friction=0.6)
+    return params, BodyArrays(bodies)
+
+
 # ---- adjoint workload --------------------------------------------------------
 
 def sliding_boxes(grid: int = 8, spacing: float = 1.5, mu: float = 0.5, e: float = 0.25, seed: int = 5,

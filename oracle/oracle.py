@@ -164,6 +164,32 @@ class PortOracle(_Oracle):
     PREFIX = "neport_"
     PATH = PORT_LIB
 
+    def __init__(self, params, bodies):
+        if np.any((bodies.shape == _ffi.MESH) | (bodies.shape == _ffi.COMPOUND)):
+            raise NotImplementedError("the C restatement has no triangle meshes or compounds; use RefOracle")
+        super().__init__(params, bodies)
+
+
+def ref_mesh(verts, tris):
+    """A triangle mesh with the reference's own BVH (MeshData::build()), as a
+    nativeengine_b200.bodies.MeshData."""
+    from nativeengine_b200.bodies import MeshData
+    lib = RefOracle.lib()
+    fn = lib.neref_mesh_build
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32] + [C.c_void_p] * 6
+    v = np.ascontiguousarray(np.asarray(verts, np.float64).reshape(-1, 3))
+    t = np.ascontiguousarray(np.asarray(tris, np.int32).reshape(-1, 3))
+    cap = 2 * len(t) + 1
+    order = np.zeros(len(t), np.int32)
+    lo, hi = np.zeros((cap, 3)), np.zeros((cap, 3))
+    ints = [np.zeros(cap, np.int32) for _ in range(4)]
+    k = fn(v.ctypes.data_as(C.c_void_p), len(v), t.ctypes.data_as(C.c_void_p), len(t),
+           order.ctypes.data_as(C.c_void_p), cap, lo.ctypes.data_as(C.c_void_p), hi.ctypes.data_as(C.c_void_p),
+           *[a.ctypes.data_as(C.c_void_p) for a in ints])
+    assert k >= 0
+    return MeshData.from_arrays(v, t, order, lo[:k], hi[:k], *[a[:k] for a in ints])
+
 
 def ref_readme_example() -> float:
     lib = RefOracle.lib()

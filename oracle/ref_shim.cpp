@@ -84,6 +84,38 @@ void loadBodies(ne::World& w, const NeBodyArrays* b) {
             for (uint32_t k = 0; k < b->vert_count[i]; ++k)
                 o.vertices.push_back(v3(b->verts, b->vert_offset[i] + k));
         }
+        if (o.shape == ne::Shape::Compound && b->child_shape) {
+            for (uint32_t k = b->child_offset[i]; k < b->child_offset[i] + b->child_count[i]; ++k) {
+                ne::ChildShape c;
+                c.shape = static_cast<ne::Shape>(b->child_shape[k]);
+                c.localPos = v3(b->child_pos, k);
+                c.localRot = ne::Q{b->child_rot[4 * k], b->child_rot[4 * k + 1], b->child_rot[4 * k + 2],
+                                   b->child_rot[4 * k + 3]};
+                c.radius = b->child_radius[k];
+                c.halfHeight = b->child_half_height[k];
+                c.halfExtents = v3(b->child_half_extents, k);
+                o.children.push_back(c);
+            }
+        }
+        if (o.shape == ne::Shape::Mesh && b->meshes) {
+            // The given BVH as ne::MeshData holds it (not rebuilt).
+            const NeMeshData& m = b->meshes[b->mesh_index[i]];
+            auto md = std::make_shared<ne::MeshData>();
+            for (uint32_t k = 0; k < m.n_verts; ++k) md->verts.push_back(v3(m.verts, k));
+            for (uint32_t k = 0; k < m.n_tris; ++k) md->tris.push_back({m.tris[3 * k], m.tris[3 * k + 1], m.tris[3 * k + 2]});
+            md->order.assign(m.order, m.order + m.n_tris);
+            for (uint32_t k = 0; k < m.n_nodes; ++k) {
+                ne::MeshData::Node nd;
+                nd.lo = v3(m.node_lo, k);
+                nd.hi = v3(m.node_hi, k);
+                nd.left = m.node_left[k];
+                nd.right = m.node_right[k];
+                nd.start = m.node_start[k];
+                nd.count = m.node_count[k];
+                md->nodes.push_back(nd);
+            }
+            o.mesh = md;
+        }
         o.friction = b->friction[i];
         o.restitution = b->restitution[i];
         o.linearDamping = b->linear_damping[i];
@@ -152,6 +184,27 @@ void* neref_create(const NeWorldParams* p, const NeBodyArrays* b) {
 }
 
 void neref_destroy(void* h) { delete static_cast<RefWorld*>(h); }
+
+// The reference's own BVH of a triangle mesh (MeshData::build(),
+// src/mesh.hpp:38-42), for giving the device the same mesh.  Returns the node
+// count, or -1 when node_cap is too small.
+int neref_mesh_build(const double* verts, uint32_t nv, const int32_t* tris, uint32_t nt, int32_t* order,
+                     uint32_t node_cap, double* lo, double* hi, int32_t* left, int32_t* right, int32_t* start,
+                     int32_t* count) {
+    ne::MeshData md;
+    for (uint32_t k = 0; k < nv; ++k) md.verts.push_back(v3(verts, k));
+    for (uint32_t k = 0; k < nt; ++k) md.tris.push_back({tris[3 * k], tris[3 * k + 1], tris[3 * k + 2]});
+    md.build();
+    if (md.nodes.size() > node_cap) return -1;
+    std::copy(md.order.begin(), md.order.end(), order);
+    for (std::size_t k = 0; k < md.nodes.size(); ++k) {
+        const ne::MeshData::Node& nd = md.nodes[k];
+        lo[3 * k] = nd.lo.x; lo[3 * k + 1] = nd.lo.y; lo[3 * k + 2] = nd.lo.z;
+        hi[3 * k] = nd.hi.x; hi[3 * k + 1] = nd.hi.y; hi[3 * k + 2] = nd.hi.z;
+        left[k] = nd.left; right[k] = nd.right; start[k] = nd.start; count[k] = nd.count;
+    }
+    return (int)md.nodes.size();
+}
 
 void neref_set_params(void* h, const NeWorldParams* p) { applyParams(static_cast<RefWorld*>(h)->w, p); }
 

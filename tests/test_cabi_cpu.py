@@ -42,11 +42,15 @@ def test_struct_layouts_match_c():
 #include "ne_cuda.h"
 #define F(T, m) printf(#T "." #m " %zu\n", offsetof(T, m))
 int main(void) {
-  printf("NeWorldParams %zu\nNeBodyArrays %zu\nNeContactArrays %zu\nNeStepStats %zu\n",
-         sizeof(NeWorldParams), sizeof(NeBodyArrays), sizeof(NeContactArrays), sizeof(NeStepStats));
+  printf("NeWorldParams %zu\nNeBodyArrays %zu\nNeContactArrays %zu\nNeStepStats %zu\nNeMeshData %zu\n",
+         sizeof(NeWorldParams), sizeof(NeBodyArrays), sizeof(NeContactArrays), sizeof(NeStepStats),
+         sizeof(NeMeshData));
   F(NeWorldParams, dt); F(NeWorldParams, gravity); F(NeWorldParams, sleep_lin_vel); F(NeWorldParams, n_joints);
   F(NeBodyArrays, x); F(NeBodyArrays, verts); F(NeBodyArrays, n_verts); F(NeBodyArrays, friction);
-  F(NeBodyArrays, n_nocollide);
+  F(NeBodyArrays, n_nocollide); F(NeBodyArrays, child_offset); F(NeBodyArrays, n_children);
+  F(NeBodyArrays, child_half_extents); F(NeBodyArrays, mesh_index); F(NeBodyArrays, n_meshes);
+  F(NeBodyArrays, meshes); F(NeMeshData, verts); F(NeMeshData, order); F(NeMeshData, n_nodes);
+  F(NeMeshData, node_count);
   return 0;
 }
 '''
@@ -62,6 +66,7 @@ int main(void) {
     assert int(got["NeBodyArrays"]) == C.sizeof(_ffi.NeBodyArrays)
     assert int(got["NeContactArrays"]) == C.sizeof(_ffi.NeContactArrays)
     assert int(got["NeStepStats"]) == C.sizeof(_ffi.NeStepStats)
+    assert int(got["NeMeshData"]) == C.sizeof(_ffi.NeMeshData)
     for key, val in got.items():
         if "." in key:
             t, m = key.split(".")
