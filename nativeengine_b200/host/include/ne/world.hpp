@@ -7,8 +7,8 @@
 // difference is where World::step() runs: the bodies are mirrored into a
 // device world (include/ne_cuda.h) and stepped on the GPU, then the state is
 // copied back into World::bodies.  Features the device path does not run
-// (joints, sleeping, CCD, meshes, compounds) make step() throw
-// ne::DeviceError instead of silently skipping them; there is no CPU path.
+// (joints, sleeping, CCD) make step() throw ne::DeviceError instead of
+// silently skipping them; there is no CPU path.
 #pragma once
 
 #include <cstdint>
@@ -26,6 +26,37 @@ namespace ne {
 
 enum class Shape { Sphere, Cylinder, Box, Capsule, Convex, Plane, Mesh, Compound };
 
+// A child primitive of a compound body in the parent's frame (src/body.hpp:28-39).
+struct ChildShape {
+    Shape shape = Shape::Sphere;
+    V3 localPos;
+    Q localRot{1, 0, 0, 0};
+    double radius = 1.0;
+    double halfHeight = 0.0;
+    V3 halfExtents;
+    static ChildShape sphere(const V3& p, double r);
+    static ChildShape box(const V3& p, const Q& q, const V3& he);
+    static ChildShape cylinder(const V3& p, const Q& q, double r, double hh);
+    static ChildShape capsule(const V3& p, const Q& q, double r, double hh);
+};
+
+// A static triangle mesh with an AABB BVH (src/mesh.hpp:14-26).  build()
+// makes the reference's tree (median split of the triangle centroids along
+// the longest axis, leaves of at most 4), so contacts come in its order.
+struct MeshData {
+    struct Tri { int a, b, c; };
+    struct Node {
+        V3 lo, hi;
+        int left = -1, right = -1;
+        int start = 0, count = 0;
+    };
+    std::vector<V3> verts;
+    std::vector<Tri> tris;
+    std::vector<int> order;
+    std::vector<Node> nodes;
+    void build();
+};
+
 struct Body {
     V3 x, v;
     Q q{1, 0, 0, 0};
@@ -38,6 +69,8 @@ struct Body {
     double halfHeight = 0.0;
     V3 halfExtents;
     std::vector<V3> vertices;
+    std::shared_ptr<const MeshData> mesh;     // Mesh only
+    std::vector<ChildShape> children;         // Compound only
     int id = -1;
     double friction = -1.0, restitution = -1.0;
     double linearDamping = 0.0, angularDamping = 0.0;
@@ -59,6 +92,8 @@ Body makeBox(int id, const V3& x, const Q& q, const V3& halfExtents, double dens
 Body makeCapsule(int id, const V3& x, const Q& q, double radius, double halfHeight, double density);
 Body makeConvex(int id, const V3& x, const Q& q, std::vector<V3> verts, double density);
 Body makePlane(int id, const V3& point, const V3& normal);
+Body makeMesh(int id, const V3& point, const Q& q, std::shared_ptr<const MeshData> data);
+Body makeCompound(int id, const V3& x, const Q& q, std::vector<ChildShape> children, double density);
 
 struct Box {
     double half = 12.0;
@@ -166,6 +201,13 @@ public:
         return add(makeConvex(0, pos, rot, verts, density));
     }
     BodyId addPlane(const V3& point, const V3& normal) { return add(makePlane(0, point, normal)); }
+    BodyId addCompound(const V3& pos, const Q& rot, const std::vector<ChildShape>& children, double density) {
+        return add(makeCompound(0, pos, rot, children, density));
+    }
+    // A static triangle mesh: verts + flat indices (triples); the BVH is built here.
+    BodyId addMesh(const V3& pos, const Q& rot, const std::vector<V3>& verts, const std::vector<int>& indices);
+    // A rows x cols height grid (row-major, spacing in x/z) as a static mesh.
+    BodyId addHeightfield(const V3& origin, double spacing, int rows, int cols, const std::vector<double>& heights);
 
     BodyId makeStatic(BodyId h);
     BodyId makeKinematic(BodyId h);

@@ -118,6 +118,154 @@ Body makePlane(int id, const V3& point, const V3& normal) {
     return b;
 }
 
+ChildShape ChildShape::sphere(const V3& p, double r) {
+    ChildShape c;
+    c.shape = Shape::Sphere; c.localPos = p; c.radius = r;
+    return c;
+}
+ChildShape ChildShape::box(const V3& p, const Q& q, const V3& he) {
+    ChildShape c;
+    c.shape = Shape::Box; c.localPos = p; c.localRot = q; c.halfExtents = he;
+    return c;
+}
+ChildShape ChildShape::cylinder(const V3& p, const Q& q, double r, double hh) {
+    ChildShape c;
+    c.shape = Shape::Cylinder; c.localPos = p; c.localRot = q; c.radius = r; c.halfHeight = hh;
+    return c;
+}
+ChildShape ChildShape::capsule(const V3& p, const Q& q, double r, double hh) {
+    ChildShape c;
+    c.shape = Shape::Capsule; c.localPos = p; c.localRot = q; c.radius = r; c.halfHeight = hh;
+    return c;
+}
+
+namespace {
+
+void tri_bounds(const MeshData& m, int t, V3& lo, V3& hi) {
+    const V3 a = m.verts[m.tris[t].a], b = m.verts[m.tris[t].b], c = m.verts[m.tris[t].c];
+    lo = {std::min({a.x, b.x, c.x}), std::min({a.y, b.y, c.y}), std::min({a.z, b.z, c.z})};
+    hi = {std::max({a.x, b.x, c.x}), std::max({a.y, b.y, c.y}), std::max({a.z, b.z, c.z})};
+}
+
+// Node over order[start, start + count): its bounds; a leaf at <= 4
+// triangles, else split at the median centroid (lo + hi) of the longest axis.
+int build_node(MeshData& m, int start, int count) {
+    const int idx = static_cast<int>(m.nodes.size());
+    m.nodes.emplace_back();
+    V3 lo{1e30, 1e30, 1e30}, hi{-1e30, -1e30, -1e30};
+    for (int k = 0; k < count; ++k) {
+        V3 tl, th;
+        tri_bounds(m, m.order[start + k], tl, th);
+        lo = {std::min(lo.x, tl.x), std::min(lo.y, tl.y), std::min(lo.z, tl.z)};
+        hi = {std::max(hi.x, th.x), std::max(hi.y, th.y), std::max(hi.z, th.z)};
+    }
+    MeshData::Node nd;
+    nd.lo = lo;
+    nd.hi = hi;
+    if (count <= 4) {
+        nd.start = start;
+        nd.count = count;
+        m.nodes[idx] = nd;
+        return idx;
+    }
+    const V3 ext = hi - lo;
+    const int axis = (ext.x > ext.y && ext.x > ext.z) ? 0 : (ext.y > ext.z ? 1 : 2);
+    auto centre = [&](int t) {
+        V3 tl, th;
+        tri_bounds(m, t, tl, th);
+        return axis == 0 ? tl.x + th.x : (axis == 1 ? tl.y + th.y : tl.z + th.z);
+    };
+    const int mid = start + count / 2;
+    std::nth_element(m.order.begin() + start, m.order.begin() + mid, m.order.begin() + start + count,
+                     [&](int p, int q) { return centre(p) < centre(q); });
+    const int l = build_node(m, start, mid - start);
+    const int r = build_node(m, mid, start + count - mid);
+    nd.left = l;
+    nd.right = r;
+    m.nodes[idx] = nd;
+    return idx;
+}
+
+}  // namespace
+
+void MeshData::build() {
+    order.resize(tris.size());
+    for (size_t k = 0; k < tris.size(); ++k) order[k] = static_cast<int>(k);
+    nodes.clear();
+    if (!tris.empty()) build_node(*this, 0, static_cast<int>(tris.size()));
+}
+
+Body makeMesh(int id, const V3& point, const Q& q, std::shared_ptr<const MeshData> data) {
+    Body b;
+    b.shape = Shape::Mesh;
+    b.id = id;
+    b.x = point;
+    b.q = q;
+    b.mesh = std::move(data);
+    b.invMass = 0.0;
+    b.invInertiaBody = {0, 0, 0};
+    b.dynamic = false;
+    return b;
+}
+
+// Mass sums the children; the inertia is the diagonal of the summed tensor by
+// the parallel-axis theorem (src/body.hpp:368-400).
+Body makeCompound(int id, const V3& x, const Q& q, std::vector<ChildShape> children, double density) {
+    Body b;
+    b.shape = Shape::Compound;
+    b.id = id;
+    b.x = x;
+    b.q = q;
+    b.children = std::move(children);
+    double M = 0.0;
+    V3 I;
+    for (const ChildShape& ch : b.children) {
+        Body t;
+        switch (ch.shape) {
+            case Shape::Box: t = makeBox(0, V3{}, Q{1, 0, 0, 0}, ch.halfExtents, density); break;
+            case Shape::Cylinder: t = makeCylinder(0, V3{}, Q{1, 0, 0, 0}, ch.radius, 2.0 * ch.halfHeight, density); break;
+            case Shape::Capsule: t = makeCapsule(0, V3{}, Q{1, 0, 0, 0}, ch.radius, ch.halfHeight, density); break;
+            default: t = makeSphere(0, V3{}, ch.radius, density); break;
+        }
+        const double mc = (t.invMass > 0) ? 1.0 / t.invMass : 0.0;
+        const V3 Ic{t.invInertiaBody.x > 0 ? 1.0 / t.invInertiaBody.x : 0.0,
+                    t.invInertiaBody.y > 0 ? 1.0 / t.invInertiaBody.y : 0.0,
+                    t.invInertiaBody.z > 0 ? 1.0 / t.invInertiaBody.z : 0.0};
+        const V3 o = ch.localPos;
+        M += mc;
+        I.x += Ic.x + mc * (o.y * o.y + o.z * o.z);
+        I.y += Ic.y + mc * (o.x * o.x + o.z * o.z);
+        I.z += Ic.z + mc * (o.x * o.x + o.y * o.y);
+    }
+    b.invMass = (M > 0) ? 1.0 / M : 0.0;
+    b.invInertiaBody = {I.x > 0 ? 1.0 / I.x : 0.0, I.y > 0 ? 1.0 / I.y : 0.0, I.z > 0 ? 1.0 / I.z : 0.0};
+    return b;
+}
+
+BodyId PhysicsWorld::addMesh(const V3& pos, const Q& rot, const std::vector<V3>& verts,
+                             const std::vector<int>& indices) {
+    auto md = std::make_shared<MeshData>();
+    md->verts = verts;
+    for (size_t k = 0; k + 2 < indices.size(); k += 3) md->tris.push_back({indices[k], indices[k + 1], indices[k + 2]});
+    md->build();
+    return add(makeMesh(0, pos, rot, md));
+}
+
+BodyId PhysicsWorld::addHeightfield(const V3& origin, double spacing, int rows, int cols,
+                                    const std::vector<double>& heights) {
+    std::vector<V3> verts;
+    for (int r = 0; r < rows; ++r)
+        for (int c = 0; c < cols; ++c)
+            verts.push_back(V3{origin.x + c * spacing, origin.y + heights[(size_t)r * cols + c], origin.z + r * spacing});
+    std::vector<int> idx;
+    for (int r = 0; r + 1 < rows; ++r)
+        for (int c = 0; c + 1 < cols; ++c) {
+            const int a = r * cols + c, b = a + 1, d = a + cols, e = d + 1;
+            idx.insert(idx.end(), {a, d, b, b, d, e});
+        }
+    return addMesh(V3{0, 0, 0}, Q{1, 0, 0, 0}, verts, idx);
+}
+
 // ---- World ----------------------------------------------------------------
 
 namespace {
@@ -154,6 +302,17 @@ struct Packed {
     std::vector<double> x, q, v, w, f, t, im, ii, r, hh, he, verts, fr, re, ld, ad, gs;
     std::vector<int32_t> shape;
     std::vector<uint32_t> vo, vc, layer, mask, flags, no, nc, nl;
+    // compound children and meshes
+    std::vector<uint32_t> co, cc, mi;
+    std::vector<int32_t> cs;
+    std::vector<double> cp, cr, crad, chh, che;
+    struct MeshArrays {
+        const MeshData* src = nullptr;
+        std::vector<double> verts, lo, hi;
+        std::vector<int32_t> tris, order, left, right, start, count;
+    };
+    std::vector<MeshArrays> marr;
+    std::vector<NeMeshData> meshes;
     NeBodyArrays view{};
 
     explicit Packed(const std::vector<Body>& B) {
@@ -186,6 +345,49 @@ struct Packed {
             no.push_back(static_cast<uint32_t>(nl.size()));
             nc.push_back(static_cast<uint32_t>(b.noCollide.size()));
             nl.insert(nl.end(), b.noCollide.begin(), b.noCollide.end());
+            co.push_back(static_cast<uint32_t>(cs.size()));
+            cc.push_back(static_cast<uint32_t>(b.children.size()));
+            for (const ChildShape& c : b.children) {
+                cs.push_back(static_cast<int32_t>(c.shape));
+                cp.insert(cp.end(), {c.localPos.x, c.localPos.y, c.localPos.z});
+                cr.insert(cr.end(), {c.localRot.w, c.localRot.x, c.localRot.y, c.localRot.z});
+                crad.push_back(c.radius);
+                chh.push_back(c.halfHeight);
+                che.insert(che.end(), {c.halfExtents.x, c.halfExtents.y, c.halfExtents.z});
+            }
+            mi.push_back(static_cast<uint32_t>(marr.size()));
+            if (b.shape == Shape::Mesh && b.mesh) {
+                const MeshData& md = *b.mesh;
+                MeshArrays a;
+                a.src = &md;
+                for (const V3& p : md.verts) a.verts.insert(a.verts.end(), {p.x, p.y, p.z});
+                for (const MeshData::Tri& t3 : md.tris) a.tris.insert(a.tris.end(), {t3.a, t3.b, t3.c});
+                a.order = md.order;
+                for (const MeshData::Node& nd : md.nodes) {
+                    a.lo.insert(a.lo.end(), {nd.lo.x, nd.lo.y, nd.lo.z});
+                    a.hi.insert(a.hi.end(), {nd.hi.x, nd.hi.y, nd.hi.z});
+                    a.left.push_back(nd.left); a.right.push_back(nd.right);
+                    a.start.push_back(nd.start); a.count.push_back(nd.count);
+                }
+                marr.push_back(std::move(a));
+            } else {
+                mi.back() = 0;
+            }
+        }
+        for (size_t k = 0; k < marr.size(); ++k) {
+            const MeshArrays& a = marr[k];
+            const MeshData& md = *a.src;
+            NeMeshData m{};
+            m.n_verts = static_cast<uint32_t>(md.verts.size());
+            m.verts = a.verts.data();
+            m.n_tris = static_cast<uint32_t>(md.tris.size());
+            m.tris = a.tris.data();
+            m.order = a.order.data();
+            m.n_nodes = static_cast<uint32_t>(md.nodes.size());
+            m.node_lo = a.lo.data(); m.node_hi = a.hi.data();
+            m.node_left = a.left.data(); m.node_right = a.right.data();
+            m.node_start = a.start.data(); m.node_count = a.count.data();
+            meshes.push_back(m);
         }
         if (verts.empty()) verts.assign(3, 0.0);
         if (nl.empty()) nl.push_back(0);
@@ -201,6 +403,17 @@ struct Packed {
         view.layer = layer.data(); view.mask = mask.data(); view.flags = flags.data();
         view.nocollide_offset = no.data(); view.nocollide_count = nc.data(); view.nocollide = nl.data();
         view.n_nocollide = static_cast<uint32_t>(nl.size());
+        if (!cs.empty()) {
+            view.child_offset = co.data(); view.child_count = cc.data();
+            view.n_children = static_cast<uint32_t>(cs.size());
+            view.child_shape = cs.data(); view.child_pos = cp.data(); view.child_rot = cr.data();
+            view.child_radius = crad.data(); view.child_half_height = chh.data(); view.child_half_extents = che.data();
+        }
+        if (!meshes.empty()) {
+            view.mesh_index = mi.data();
+            view.n_meshes = static_cast<uint32_t>(meshes.size());
+            view.meshes = meshes.data();
+        }
     }
 };
 

@@ -62,6 +62,38 @@ int main() {
         check(a.x == b.x && a.y == b.y && a.z == b.z, "determinism: identical runs are bit-identical");
         check(run(true).norm() > 0.0, "remove: swap-and-pop keeps handles valid");
     }
+    {   // a sphere and a box on a two-triangle floor mesh (the reference's mesh self-test setting)
+        ne::PhysicsWorld pw;
+        pw.setBox(1000.0, false);
+        pw.setTimestep(1.0 / 240.0);
+        pw.setGravity(ne::V3{0, -10, 0});
+        pw.setRestitution(0.0);
+        pw.setFriction(0.5);
+        pw.addMesh(ne::V3{0, 0, 0}, ne::Q{1, 0, 0, 0}, {{-10, 0, -10}, {10, 0, -10}, {10, 0, 10}, {-10, 0, 10}},
+                   {0, 1, 2, 0, 2, 3});
+        ne::BodyId ball = pw.addSphere(ne::V3{1, 5, 1}, 0.5, 1.0);
+        ne::BodyId bx = pw.addBox(ne::V3{-3, 5, -2}, ne::Q{1, 0, 0, 0}, ne::V3{0.5, 0.5, 0.5}, 1.0);
+        pw.world().stepDevice(1500);
+        pw.world().syncFromDevice();
+        check(std::fabs(pw.position(ball).y - 0.5) < 0.05, "mesh: sphere rests on the mesh floor");
+        check(std::fabs(pw.position(bx).y - 0.5) < 0.08, "mesh: box rests on the mesh floor");
+    }
+    {   // a dumbbell compound on a floor box (the reference's compound self-test setting)
+        ne::PhysicsWorld pw;
+        pw.setBox(1000.0, false);
+        pw.setTimestep(1.0 / 240.0);
+        pw.setGravity(ne::V3{0, -10, 0});
+        pw.setRestitution(0.0);
+        pw.setFriction(0.5);
+        pw.makeStatic(pw.addBox(ne::V3{0, -1, 0}, ne::Q{1, 0, 0, 0}, ne::V3{20, 1, 20}, 1.0));
+        ne::BodyId db = pw.addCompound(ne::V3{0, 5, 0}, ne::Q{1, 0, 0, 0},
+                                       {ne::ChildShape::sphere(ne::V3{-1, 0, 0}, 0.5),
+                                        ne::ChildShape::sphere(ne::V3{1, 0, 0}, 0.5)}, 1.0);
+        pw.world().stepDevice(1500);
+        pw.world().syncFromDevice();
+        check(std::fabs(pw.position(db).y - 0.5) < 0.05, "compound: dumbbell rests on both spheres");
+        check(pw.velocity(db).norm() < 0.1, "compound: comes to rest");
+    }
     std::printf("%d failed\n", g_fail);
     return g_fail == 0 ? 0 : 1;
 }
