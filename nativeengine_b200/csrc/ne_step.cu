@@ -748,7 +748,7 @@ __device__ __forceinline__ bool sphere_pass(const CullA& A, const D4& s) {
     return !(norm2(dd) > r * r);
 }
 
-__global__ void __launch_bounds__(kT, 3) k_surv_gather(StepArgs a, int kb) {
+__global__ void __launch_bounds__(kT, 5) k_surv_gather(StepArgs a, int kb) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     __shared__ uint32_t s_lo[kT / 32][28], s_len[kT / 32][28], s_ex[kT / 32][29];
