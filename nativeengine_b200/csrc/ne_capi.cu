@@ -194,7 +194,9 @@ int alloc_scratch(NeWorld* w) {
     uint64_t scann = std::max<uint64_t>(w->Scap, std::max<uint64_t>(hw, sortn));
     int rc;
     if ((rc = dalloc(&d.hist, hw)) != NE_OK) return rc;
-    if ((rc = dalloc(&d.tsum, neb::scan_tsum_words((uint32_t)scann) + 8)) != NE_OK) return rc;
+    const size_t tw = neb::scan_tsum_words((uint32_t)scann) + 8;
+    if ((rc = dalloc(&d.tsum, tw)) != NE_OK) return rc;
+    NE_CUDA_TRY(cudaMemset(d.tsum, 0, tw * sizeof(uint32_t)));   // scan tile states start empty
     return NE_OK;
 }
 

@@ -1,7 +1,7 @@
 // ne_prims.cu -- device-wide exclusive scan and stable LSD radix sort.
 //
 // Both are HBM-streaming primitives written for deterministic output: the scan
-// is a three-phase tile scan, and the sort ranks elements inside each 256-item
+// is a single-pass tile scan with chained tile prefixes, and the sort ranks elements inside each 256-item
 // warp sub-tile with __match_any_sync in element order, so equal keys keep
 // their input order (stability is what keeps bodies in a cell, and contacts in
 // an island, in the reference's index order).
@@ -9,6 +9,8 @@
 // Both take a host-side capacity n (launch size) and an optional device-side
 // count n_dev: only the first min(n, *n_dev) elements are scanned or sorted,
 // so a buffer sized for the worst case costs only what the step filled.
+#include <cuda/atomic>
+
 #include "ne_internal.cuh"
 
 namespace neb {
@@ -18,7 +20,6 @@ namespace {
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;   // 2048
-constexpr int kTopThreads = 1024;
 
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
     const int lane = threadIdx.x & 31;
@@ -56,64 +57,99 @@ __device__ __forceinline__ uint32_t live_count(uint32_t n, const uint64_t* n_dev
     return v < (uint64_t)n ? (uint32_t)v : n;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t* __restrict__ in,
-                                                             uint32_t* __restrict__ out, uint32_t ncap,
-                                                             uint32_t* __restrict__ tsum,
+// Single-pass exclusive scan: tiles take numbers from a ticket in the order
+// they start, publish their sum, then walk back over earlier tiles' published
+// sums to the first one that carries its inclusive prefix (chained tile
+// prefixes).  A tile only waits on tiles that started before it, so every wait
+// ends; it is still bounded in time, and reports through ctl->solve_timeout.
+// The last tile to finish clears the tile states and counters for the next
+// scan (scans on one stream never overlap).
+//   tstat[0, ntiles): (flag << 62) | value, flag 1 = tile sum, 2 = inclusive
+//   prefix; the two u32 words after them: ticket and finished count.
+constexpr unsigned long long kTileSum = 1ull << 62, kTilePrefix = 2ull << 62, kTileVal = (1ull << 62) - 1;
+constexpr unsigned long long kLookbackNs = 2000000000ull;
+
+__device__ __forceinline__ unsigned long long scan_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_1pass(const uint32_t* in, uint32_t* out, uint32_t ncap,
+                                                             unsigned long long* __restrict__ tstat,
+                                                             uint32_t ntiles_cap, uint64_t* __restrict__ total,
                                                              const Ctl* __restrict__ ctl,
                                                              const uint64_t* __restrict__ n_dev) {
     if (ctl->abort) return;
     __shared__ uint32_t sm[33];
-    const uint32_t n = live_count(ncap, n_dev);
-    if ((uint64_t)blockIdx.x * kScanTile >= n) {
-        if (threadIdx.x == 0) tsum[blockIdx.x] = 0u;
-        return;
-    }
-    const uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
-    uint32_t x[kScanItems];
-    uint32_t s = 0;
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        x[k] = (base + k < n) ? in[base + k] : 0u;
-        s += x[k];
-    }
-    uint32_t excl;
-    uint32_t total = block_excl_scan<kScanThreads>(s, excl, sm);
-#pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < n) out[base + k] = excl;
-        excl += x[k];
-    }
-    if (threadIdx.x == 0) tsum[blockIdx.x] = total;
-}
-
-// Single block: exclusive scan of the tile sums, u64 grand total.
-__global__ void __launch_bounds__(kTopThreads) k_scan_top(uint32_t* __restrict__ tsum, uint32_t ntiles,
-                                                          uint64_t* __restrict__ total,
-                                                          const Ctl* __restrict__ ctl) {
-    if (ctl->abort) return;
-    __shared__ uint32_t sm[33];
-    __shared__ unsigned long long carry;
-    if (threadIdx.x == 0) carry = 0ull;
+    __shared__ uint32_t s_tile, s_last;
+    __shared__ unsigned long long s_prefix;
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(tstat + ntiles_cap);
+    if (threadIdx.x == 0) s_tile = atomicAdd(&ctr[0], 1u);
     __syncthreads();
-    for (uint32_t base = 0; base < ntiles; base += kTopThreads) {
-        const uint32_t idx = base + threadIdx.x;
-        uint32_t v = (idx < ntiles) ? tsum[idx] : 0u;
-        uint32_t excl;
-        uint32_t t = block_excl_scan<kTopThreads>(v, excl, sm);
-        if (idx < ntiles) tsum[idx] = (uint32_t)(carry + excl);
-        __syncthreads();
-        if (threadIdx.x == 0) carry += t;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *total = carry;
-}
-
-__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t ncap, const uint32_t* __restrict__ tsum,
-                           const Ctl* __restrict__ ctl, const uint64_t* __restrict__ n_dev) {
-    if (ctl->abort) return;
+    const uint32_t tile = s_tile;
     const uint32_t n = live_count(ncap, n_dev);
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] += tsum[i / kScanTile];
+    const uint32_t live = (uint32_t)(((uint64_t)n + kScanTile - 1) / kScanTile);
+    using Word = cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>;
+    if (tile < live) {
+        const uint64_t base = (uint64_t)tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+        uint32_t x[kScanItems];
+        uint32_t sum = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            x[k] = (base + k < n) ? in[base + k] : 0u;
+            sum += x[k];
+        }
+        uint32_t excl;
+        const uint32_t tot = block_excl_scan<kScanThreads>(sum, excl, sm);
+        if (threadIdx.x == 0) {
+            unsigned long long prefix = 0;
+            if (tile == 0) {
+                Word(tstat[0]).store(kTilePrefix | tot, cuda::memory_order_relaxed);
+            } else {
+                Word(tstat[tile]).store(kTileSum | tot, cuda::memory_order_relaxed);
+                const unsigned long long t0 = scan_ns();
+                uint32_t spins = 0;
+                for (int64_t q = (int64_t)tile - 1; q >= 0;) {
+                    const unsigned long long v = Word(tstat[q]).load(cuda::memory_order_relaxed);
+                    const unsigned long long f = v & ~kTileVal;
+                    if (f == 0ull) {
+                        if ((++spins & 255u) == 0u && scan_ns() - t0 > kLookbackNs) {
+                            atomicExch(const_cast<uint32_t*>(&ctl->solve_timeout), 1u);
+                            break;
+                        }
+                        continue;
+                    }
+                    prefix += v & kTileVal;
+                    if (f == kTilePrefix) break;
+                    --q;
+                }
+                Word(tstat[tile]).store(kTilePrefix | (prefix + tot), cuda::memory_order_relaxed);
+            }
+            s_prefix = prefix;
+            if (tile == live - 1) *total = prefix + tot;
+        }
+        __syncthreads();
+        excl += (uint32_t)s_prefix;
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) {
+            if (base + k < n) out[base + k] = excl;
+            excl += x[k];
+        }
+    } else if (n == 0 && tile == 0 && threadIdx.x == 0) {
+        *total = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = (atomicAdd(&ctr[1], 1u) == gridDim.x - 1) ? 1u : 0u;
+    }
+    __syncthreads();
+    if (s_last) {
+        for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) tstat[k] = 0ull;
+        if (threadIdx.x == 0) { ctr[0] = 0u; ctr[1] = 0u; }
+        __threadfence();
+    }
 }
 
 // ---- radix sort ---------------------------------------------------------
@@ -218,20 +254,17 @@ int radix_sort_impl(K* key[2], uint32_t* val[2], uint32_t n, int bits, uint32_t*
 
 }  // namespace
 
-size_t scan_tsum_words(uint32_t n) { return (size_t)ceil_div(n, kScanTile) + 1; }
+// u32 words of scan state: one u64 per tile, then the two counters.
+size_t scan_tsum_words(uint32_t n) { return 2 * ((size_t)ceil_div(n ? n : 1, kScanTile) + 2); }
 size_t radix_hist_words(uint32_t n) { return (size_t)256 * ceil_div(n, kSub) + 1; }
 
 void scan_u32(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tsum, uint64_t* total, const Ctl* ctl,
               cudaStream_t st, uint64_t* launches, const uint64_t* n_dev) {
     if (n == 0) return;
     const uint32_t ntiles = ceil_div(n, kScanTile);
-    k_scan_tiles<<<ntiles, kScanThreads, 0, st>>>(in, out, n, tsum, ctl, n_dev);
-    k_scan_top<<<1, kTopThreads, 0, st>>>(tsum, ntiles, total, ctl);
-    *launches += 2;
-    if (ntiles > 1) {
-        k_scan_add<<<ceil_div(n, 256), 256, 0, st>>>(out, n, tsum, ctl, n_dev);
-        ++*launches;
-    }
+    k_scan_1pass<<<ntiles, kScanThreads, 0, st>>>(in, out, n, reinterpret_cast<unsigned long long*>(tsum), ntiles,
+                                                  total, ctl, n_dev);
+    ++*launches;
 }
 
 int radix_sort_u64(unsigned long long* key[2], uint32_t* val[2], uint32_t n, int bits, uint32_t* hist,
