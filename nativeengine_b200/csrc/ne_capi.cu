@@ -65,6 +65,7 @@ struct NeWorld {
     NeWorldParams p{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    neb::SideStream side{};               // small-island solve beside the big-island solvers
     uint32_t n = 0;
     neb::DevWorld d{};
     neb::Ctl* h_ctl = nullptr;   // pinned mirror of d.ctl
@@ -466,6 +467,9 @@ int ne_world_create(const NeWorldParams* params, NeWorld** out) {
     NE_CUDA_TRY(cudaGetDevice(&w->device));
     NE_CUDA_TRY(cudaDeviceGetAttribute(&w->num_sms, cudaDevAttrMultiProcessorCount, w->device));
     NE_CUDA_TRY(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+    NE_CUDA_TRY(cudaStreamCreateWithFlags(&w->side.st2, cudaStreamNonBlocking));
+    NE_CUDA_TRY(cudaEventCreateWithFlags(&w->side.fork, cudaEventDisableTiming));
+    NE_CUDA_TRY(cudaEventCreateWithFlags(&w->side.join, cudaEventDisableTiming));
     neb::init_kernel_attrs();
     NE_CUDA_TRY(cudaGetLastError());
     NE_CUDA_TRY(cudaMallocHost((void**)&w->h_ctl, sizeof(neb::Ctl)));
@@ -494,6 +498,10 @@ int ne_world_destroy(NeWorld* w) {
     for (int k = 0; k <= NE_NUM_STAGES; ++k)
         if (w->ev[k]) cudaEventDestroy(w->ev[k]);
     if (w->gexec) cudaGraphExecDestroy(w->gexec);
+    if (w->side.st2) cudaStreamSynchronize(w->side.st2);
+    if (w->side.fork) cudaEventDestroy(w->side.fork);
+    if (w->side.join) cudaEventDestroy(w->side.join);
+    if (w->side.st2) cudaStreamDestroy(w->side.st2);
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
     return NE_OK;
@@ -896,7 +904,7 @@ int step_eager(NeWorld* w, int* status) {
     for (int attempt = 0;; ++attempt) {
         if (attempt > 16) return set_err(NE_ERR_CAPACITY, "step did not fit after repeated growth");
         neb::StepArgs a = make_args(w);
-        neb::launch_step(a, w->stream, &w->launches, w->profile ? w->ev : nullptr);
+        neb::launch_step(a, w->stream, &w->launches, w->profile ? w->ev : nullptr, &w->side);
         NE_CUDA_TRY(cudaGetLastError());
         NE_CUDA_TRY(cudaMemcpyAsync(w->h_ctl, w->d.ctl, sizeof(neb::Ctl), cudaMemcpyDeviceToHost, w->stream));
         NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
@@ -949,7 +957,7 @@ int step_graph_batch(NeWorld* w, uint32_t want, uint32_t* done, bool* halted, in
         uint64_t L = 0;
         cudaGraph_t g = nullptr;
         NE_CUDA_TRY(cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal));
-        neb::launch_step(a, w->stream, &L, nullptr);
+        neb::launch_step(a, w->stream, &L, nullptr, &w->side);
         const cudaError_t le = cudaGetLastError();
         const cudaError_t ce = cudaStreamEndCapture(w->stream, &g);
         if (le != cudaSuccess || ce != cudaSuccess) {

@@ -81,8 +81,11 @@ __device__ __forceinline__ uint32_t big_successor(const DevWorld& d, const uint3
 // correction (:615-616), warm-cache values (:619-626).  Islands share no
 // mutable body, so concurrent islands reproduce the reference's single
 // global sweep exactly.  Big islands are queued for the dataflow solvers.
-template <class Items>
-__device__ __forceinline__ void island_solve_small(const StepArgs& a, int ib) {
+//
+// island_list (one thread per island) records the largest island and lists
+// the big ones with their size classes first, so that the big-island solvers
+// and the small-island solve can run side by side.
+__device__ __forceinline__ void island_list(const StepArgs& a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -94,8 +97,18 @@ __device__ __forceinline__ void island_solve_small(const StepArgs& a, int ib) {
         const uint32_t slot = atomicAdd(&ctl->nbig, 1u);
         d.big[slot] = (uint32_t)t;
         atomicAdd(&ctl->big_class[31 - __clz(e - s)], 1u);
-        return;
     }
+}
+
+template <class Items>
+__device__ __forceinline__ void island_solve_small(const StepArgs& a, int ib) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ctl->islands) return;
+    const DevWorld& d = a.d;
+    const uint32_t s = d.istart[t], e = d.istart[t + 1];
+    if (e - s >= kBigIsland) return;   // listed for the dataflow solvers
     const uint32_t* ord = d.iord[ib];
     if (a.warm)
         for (uint32_t k = s; k < e; ++k) Items::warm(d, ord[k]);

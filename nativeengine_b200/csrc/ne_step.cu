@@ -1428,6 +1428,8 @@ struct ItemsF64 {
 
 };
 
+__global__ void __launch_bounds__(128) k_island_list(StepArgs a) { solve::island_list(a); }
+
 __global__ void __launch_bounds__(128) k_island_solve(StepArgs a, int ib) {
     solve::island_solve_small<ItemsF64<false>>(a, ib);
 }
@@ -1595,7 +1597,7 @@ void init_kernel_attrs() {
 
 // Enqueue one step.  The host reads ctl afterwards to learn whether it must
 // be re-run with larger buffers.
-void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEvent_t* ev) {
+void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEvent_t* ev, const SideStream* side) {
     StepArgs a = a0;
     const DevWorld& d = a.d;
     Ctl* ctl = d.ctl;
@@ -1674,10 +1676,18 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
                                   &ctl->C2);
     k_rank_write<<<blocks_for(2 * a.Ccap, kT), kT, 0, st>>>(a, rb); ++L;
     mark(6);
+    k_island_list<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a); ++L;
+    // Small islands (one thread each) on the side stream, beside the big ones.
+    cudaStream_t ss = st;
+    if (side && side->st2) {
+        cudaEventRecord(side->fork, st);
+        cudaStreamWaitEvent(side->st2, side->fork, 0);
+        ss = side->st2;
+    }
     if (a.f32) {
-        launch_solve_f32(a, ib, rb, st, launches);
+        launch_solve_f32(a, ib, rb, st, ss, launches);
     } else {
-        k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib); ++L;
+        k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, ss>>>(a, ib); ++L;
         if (a.big_team_max == 1) {
             launch_big_rec(a, ib, rb, st, launches);
             k_island_solve_shared<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, a.local_cap, st>>>(a); ++L;
@@ -1687,6 +1697,11 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
             k_island_solve_big<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb); ++L;
         }
     }
+    if (ss != st) {
+        cudaEventRecord(side->join, ss);
+        cudaStreamWaitEvent(st, side->join, 0);
+    }
+    if (a.f32) launch_writeback_f32(a, st, launches);
     mark(7);
     k_boundary<<<blocks_for(a.n, kT), kT, 0, st>>>(a); ++L;
     k_step_end<<<1, 1, 0, st>>>(a); ++L;

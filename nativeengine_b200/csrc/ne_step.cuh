@@ -61,10 +61,19 @@ constexpr uint32_t kLocalCap = 65536;
 void init_kernel_attrs();
 void init_kernel_attrs_f32();
 
+// A second stream and two events: the small-island solve runs on st2 beside
+// the big-island solvers on the main stream (fork after the island list, join
+// before the boundary).  st2 == nullptr runs everything on the main stream.
+struct SideStream {
+    cudaStream_t st2;
+    cudaEvent_t fork, join;
+};
+
 // ev: NE_NUM_STAGES + 1 events recorded at the stage boundaries, or nullptr.
 // Grid shapes depend on the capacities in a only (live counts are read on the
 // device), so the enqueued step can be captured once and replayed.
-void launch_step(const StepArgs& a, cudaStream_t st, uint64_t* launches, cudaEvent_t* ev);
+void launch_step(const StepArgs& a, cudaStream_t st, uint64_t* launches, cudaEvent_t* ev,
+                 const SideStream* side = nullptr);
 // Clears the batch fields of ctl (halt, steps_done, accumulators) before a
 // replayed batch of steps.
 void launch_batch_begin(Ctl* ctl, cudaStream_t st);
@@ -72,7 +81,10 @@ void launch_batch_begin(Ctl* ctl, cudaStream_t st);
 // FP32 stages (ne_step_f32.cu), enqueued by launch_step when a.f32 is set;
 // the FP64 constraint build writes the FP32 solver records itself.
 void launch_narrowphase_f32(const StepArgs& a, cudaStream_t st, uint64_t* launches);
-void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches);
+// small: the stream of the small-island solve (the main stream or the side one).
+void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, cudaStream_t small, uint64_t* launches);
+// FP32 velocities back into the FP64 state, after both solves.
+void launch_writeback_f32(const StepArgs& a, cudaStream_t st, uint64_t* launches);
 // Teams and dataflow state of the big islands (ne_step.cu; both precisions).
 void launch_big_prep(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launches);
 // Per-position records of the big islands for the shared-memory solver.
