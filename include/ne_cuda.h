@@ -18,9 +18,8 @@
  *  - Vectors are interleaved: x[3*i+0..2]; quaternions are (w,x,y,z) like ne::Q
  *    (src/vmath.hpp:47-48).
  *  - Features that the reference supports but this device path does not yet run
- *    (joints, sleeping, CCD; triangle meshes and compounds in the FP32 form)
- *    make ne_world_upload / ne_world_step return NE_ERR_UNSUPPORTED.  There is
- *    no CPU fallback.
+ *    (joints, sleeping, CCD) make ne_world_upload / ne_world_step return
+ *    NE_ERR_UNSUPPORTED.  There is no CPU fallback.
  */
 #ifndef NE_CUDA_H
 #define NE_CUDA_H

@@ -648,8 +648,6 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
     for (uint32_t i = 0; i < n; ++i) {
         const int s = b->shape[i];
         if (s < 0 || s > NE_SHAPE_COMPOUND) return set_err(NE_ERR_ARG, "shape tag out of range");
-        if ((s == NE_SHAPE_MESH || s == NE_SHAPE_COMPOUND) && w->precision == NE_PRECISION_F32)
-            return set_err(NE_ERR_UNSUPPORTED, "triangle meshes and compounds are not in the FP32 form");
         if (s == NE_SHAPE_COMPOUND) {
             if (!b->child_offset || !b->child_count || !b->child_shape || !b->child_pos || !b->child_rot ||
                 !b->child_radius || !b->child_half_height || !b->child_half_extents)
@@ -1223,8 +1221,6 @@ int ne_world_set_precision(NeWorld* w, int precision) {
     NE_CUDA_TRY(cudaSetDevice(w->device));
     NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
     if (precision == w->precision) return NE_OK;
-    if (precision == NE_PRECISION_F32 && w->has_ext)
-        return set_err(NE_ERR_UNSUPPORTED, "triangle meshes and compounds are not in the FP32 form");
     w->precision = precision;
     int rc;
     if (precision == NE_PRECISION_F32) {

@@ -1031,6 +1031,26 @@ __device__ void ext_contacts(const DevWorld& d, uint32_t i, uint32_t j, const Bo
     }
 }
 
+// Contact counts of the mesh and compound pairs alone (the FP32 form, whose
+// narrowphase leaves those pairs to the FP64 passes).
+__global__ void __launch_bounds__(128) k_narrowphase_ext_count(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ctl->S) return;
+    const DevWorld& d = a.d;
+    const uint32_t i = d.si[s], j = d.sj[s];
+    if (!is_ext_shape((int)d.meta[i].x) && !is_ext_shape((int)d.meta[j].x)) return;
+    const BodyG A = load_geom(d, i), B = load_geom(d, j);
+    EpaScratch S;
+    int fl = 0;
+    ExtOut out{nullptr, nullptr, 0, 0, false};
+    ext_contacts(d, i, j, A, B, a.wp[a.bw[i]].dom, S, fl, out);
+    d.ccnt[s] = out.n;
+    if (fl & 1) atomicOr(&ctl->flags, 1u);
+    if (fl & 2) atomicAdd((unsigned long long*)&ctl->epa_cap_hits, 1ull);
+}
+
 // Second pass over the mesh and compound pairs: their contacts at their
 // constraint index.
 __global__ void __launch_bounds__(128) k_narrowphase_ext(StepArgs a) {
@@ -1647,6 +1667,9 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
     mark(3);
     if (a.f32) {
         launch_narrowphase_f32(a, st, launches);
+        if (a.any_ext) {
+            k_narrowphase_ext_count<<<blocks_for(a.Scap, 128), 128, 0, st>>>(a); ++L;
+        }
     } else {
         k_narrowphase<<<blocks_for(a.Scap, 128), 128, 0, st>>>(a); ++L;
     }

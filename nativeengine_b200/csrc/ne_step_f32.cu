@@ -64,6 +64,10 @@ __global__ void __launch_bounds__(128) k_narrowphase_f32(StepArgs a) {
     if (s >= ctl->S) return;
     const DevWorld& d = a.d;
     const uint32_t i = d.si[s], j = d.sj[s];
+    // Triangle meshes and compounds: their contacts come from the FP64
+    // count and write passes (k_narrowphase_ext_count, k_narrowphase_ext).
+    const int shi = (int)d.meta[i].x, shj = (int)d.meta[j].x;
+    if (shi == SH_MESH || shi == SH_COMPOUND || shj == SH_MESH || shj == SH_COMPOUND) return;
     const Domain dom = a.wp[a.bw[i]].dom;
     const V3 xi = v3d(d.pos[i]), xj = v3d(d.pos[j]);
     const V3 dij = min_image(dom, xj - xi);

@@ -33,6 +33,8 @@ SCENES = {
     "box_stack": (lambda: scenes.box_stack(levels=6), 120),
     "granular_2048": (lambda: scenes.granular_mix(n=2048, max_attempts=2000, seed=7), 10),
     "batch_24": (_batch_small, 60),
+    "compound_pile": (lambda: scenes.compound_pile(), 120),
+    "terrain_drop": (lambda: scenes.terrain_drop(), 120),
 }
 
 

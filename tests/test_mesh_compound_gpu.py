@@ -2,7 +2,7 @@
 in place (gatherContacts / meshContacts, src/world.cpp:53-121): pair lists,
 contact lists (one per overlapping triangle, one per touching child), island
 partitions and poses, bit for bit; and the same worlds in a batch, through the
-CUDA graph, and refused by the FP32 form."""
+CUDA graph, and in the FP32 form."""
 import numpy as np
 import pytest
 
@@ -125,10 +125,17 @@ def test_graph_and_eager_agree_with_meshes_and_compounds():
 
 
 @pytest.mark.gpu
-def test_fp32_form_refuses_meshes_and_compounds():
-    params, bodies = scenes.compound_pile(n=4)
-    dev = DeviceWorld(params, bodies, record=False)
-    with pytest.raises(_ffi.NeError) as e:
-        dev.set_precision("f32")
-    assert e.value.code == _ffi.NE_ERR_UNSUPPORTED
-    dev.close()
+def test_fp32_form_steps_meshes_and_compounds_graph_and_eager_alike():
+    """The FP32 form takes mesh and compound contacts from the FP64 passes;
+    graph-replayed and kernel-by-kernel FP32 steps agree bit for bit."""
+    out = []
+    for graph in (True, False):
+        params, bodies = scenes.compound_pile(n=10, with_mesh=True)
+        dev = DeviceWorld(params, bodies, record=False, precision="f32")
+        dev.set_graph(graph)
+        dev.step(120)
+        assert dev.stats()["contacts"] > 0
+        out.append(dev.state())
+        dev.close()
+    for key in ("x", "q", "v", "w"):
+        assert np.array_equal(out[0][key], out[1][key]), key
