@@ -1691,6 +1691,20 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
     k_island_mark<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a, ib); ++L;
     scan_u32(d.iflag, d.ioff, (uint32_t)a.Ccap, d.tsum, &ctl->scan_total, ctl, st, launches, &ctl->C);
     k_island_start<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a); ++L;
+    k_island_list<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a); ++L;
+    // Small islands (one thread each) on the side stream, beside the rank
+    // sort and the big-island solvers.
+    cudaStream_t ss = st;
+    if (side && side->st2) {
+        cudaEventRecord(side->fork, st);
+        cudaStreamWaitEvent(side->st2, side->fork, 0);
+        ss = side->st2;
+    }
+    if (a.f32) {
+        launch_solve_small_f32(a, ib, ss, launches);
+    } else {
+        k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, ss>>>(a, ib); ++L;
+    }
     // Per-body update ranks for the dataflow solver.
     k_rank_entries<<<blocks_for(a.Ccap, kT), kT, 0, st>>>(a, ib); ++L;
     uint32_t* rks[2] = {d.rkey[0], d.rkey[1]};
@@ -1699,18 +1713,9 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
                                   &ctl->C2);
     k_rank_write<<<blocks_for(2 * a.Ccap, kT), kT, 0, st>>>(a, rb); ++L;
     mark(6);
-    k_island_list<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a); ++L;
-    // Small islands (one thread each) on the side stream, beside the big ones.
-    cudaStream_t ss = st;
-    if (side && side->st2) {
-        cudaEventRecord(side->fork, st);
-        cudaStreamWaitEvent(side->st2, side->fork, 0);
-        ss = side->st2;
-    }
     if (a.f32) {
-        launch_solve_f32(a, ib, rb, st, ss, launches);
+        launch_solve_big_f32(a, ib, rb, st, launches);
     } else {
-        k_island_solve<<<blocks_for(a.Ccap, 128), 128, 0, ss>>>(a, ib); ++L;
         if (a.big_team_max == 1) {
             launch_big_rec(a, ib, rb, st, launches);
             k_island_solve_shared<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, a.local_cap, st>>>(a); ++L;

@@ -81,8 +81,9 @@ void launch_batch_begin(Ctl* ctl, cudaStream_t st);
 // FP32 stages (ne_step_f32.cu), enqueued by launch_step when a.f32 is set;
 // the FP64 constraint build writes the FP32 solver records itself.
 void launch_narrowphase_f32(const StepArgs& a, cudaStream_t st, uint64_t* launches);
-// small: the stream of the small-island solve (the main stream or the side one).
-void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, cudaStream_t small, uint64_t* launches);
+// Small islands (one thread each) and big islands (dataflow solvers).
+void launch_solve_small_f32(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launches);
+void launch_solve_big_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches);
 // FP32 velocities back into the FP64 state, after both solves.
 void launch_writeback_f32(const StepArgs& a, cudaStream_t st, uint64_t* launches);
 // Teams and dataflow state of the big islands (ne_step.cu; both precisions).

@@ -281,8 +281,12 @@ void launch_narrowphase_f32(const StepArgs& a, cudaStream_t st, uint64_t* launch
     ++*launches;
 }
 
-void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, cudaStream_t small, uint64_t* launches) {
-    k_island_solve_f32<<<blocks_for(a.Ccap, 128), 128, 0, small>>>(a, ib);
+void launch_solve_small_f32(const StepArgs& a, int ib, cudaStream_t st, uint64_t* launches) {
+    k_island_solve_f32<<<blocks_for(a.Ccap, 128), 128, 0, st>>>(a, ib);
+    ++*launches;
+}
+
+void launch_solve_big_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, uint64_t* launches) {
     if (a.big_team_max == 1) {
         launch_big_rec(a, ib, rb, st, launches);
         k_island_solve_shared_f32<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, a.local_cap, st>>>(a);
@@ -292,7 +296,7 @@ void launch_solve_f32(const StepArgs& a, int ib, int rb, cudaStream_t st, cudaSt
         launch_big_prep(a, ib, st, launches);
         k_island_solve_big_f32<<<a.num_sms * a.big_ctas_per_sm, a.big_threads, 0, st>>>(a, ib, rb);
     }
-    *launches += 2;
+    ++*launches;
 }
 
 void launch_writeback_f32(const StepArgs& a, cudaStream_t st, uint64_t* launches) {
