@@ -324,7 +324,7 @@ int ne_checkpoint_destroy(NeCheckpoint* checkpoint);
  * x, q, v, w), dL/d per-body mass (inverse inertia scaled with the mass, shape
  * fixed), dL/d per-body inverse mass and inverse inertia, and dL/d per-world
  * friction and restitution (through the bodies that inherit the world's
- * values).  Every step is recomputed on the device, one warp per world,
+ * values).  Every step is recomputed on the device, one CTA per world,
  * from states checkpointed every `checkpoint_every` steps (0 = one segment);
  * the contact set, clamps and branches are those of the trajectory, so the
  * result is the derivative of the piecewise-smooth map on the piece the

@@ -1,5 +1,5 @@
-// ne_adjoint.cu -- stepBackward on the device: one warp per world runs the
-// per-world step program and its adjoint (ne_adjoint.cuh), its lanes sharing
+// ne_adjoint.cu -- stepBackward on the device: one CTA per world runs the
+// per-world step program and its adjoint (ne_adjoint.cuh), its threads sharing
 // the bodies, the pairs and the islands of the world.
 //
 // Per world: (1) the state and the warm-cache entries of the world are read
@@ -53,13 +53,16 @@ __device__ __forceinline__ void copy_warm(const WarmSlot& dst, const WarmSlot& s
     t.sync();
 }
 
-constexpr int kWarpsPerBlock = 2;
+// Threads per world: the lanes share the world's bodies, pairs, islands and
+// contacts; 64 keeps every world of a 512-world batch resident at once.
+constexpr int kTeamThreads = 64;
 
-// One warp per world.
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_adj_world(AdjArgs a) {
-    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (w >= a.nworlds) return;   // whole warps only
-    const adj::Team t{(int)(threadIdx.x & 31), 32};
+// One CTA per world.
+__global__ void __launch_bounds__(kTeamThreads) k_adj_world(AdjArgs a) {
+    __shared__ uint32_t s_team[adj::kTeamScratch];
+    const uint32_t w = blockIdx.x;
+    if (w >= a.nworlds) return;   // whole blocks only
+    const adj::Team t{(int)threadIdx.x, (int)blockDim.x, s_team};
     const DevWorld& d = a.d;
     const WorldP& W = a.wp[w];
     const uint32_t b0 = a.wbegin[w], b1 = a.wbegin[w + 1], nb = b1 - b0;
@@ -217,7 +220,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_adj_world(AdjArgs a) {
 }  // namespace
 
 void launch_adjoint(const AdjArgs& a, cudaStream_t st) {
-    k_adj_world<<<(a.nworlds + kWarpsPerBlock - 1) / kWarpsPerBlock, 32 * kWarpsPerBlock, 0, st>>>(a);
+    k_adj_world<<<a.nworlds, kTeamThreads, 0, st>>>(a);
 }
 
 }  // namespace neb

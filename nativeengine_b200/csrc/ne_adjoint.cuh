@@ -24,7 +24,8 @@
 // box-box normal comes from EPA's final face, rebuilt from its box corners.
 //
 // Everything is __host__ __device__: the device kernel (ne_adjoint.cu) runs it
-// one warp per world (a Team of 32); the host test build runs a Team of one.
+// one CTA per world (a Team of its threads); the host test build runs a Team
+// of one.
 #pragma once
 
 #include "ne_dual.cuh"
@@ -400,21 +401,38 @@ struct WScr {
 // lanes; each island's solver updates run on one lane, in order.
 struct Team {
     int lane, size;
+    // Block teams (size > 32): shared scratch of kTeamScratch words; a warp
+    // (size 32) or the host build (size 1) needs none.
+    uint32_t* sm = nullptr;
     NE_HD void sync() const {
 #ifdef __CUDA_ARCH__
-        __syncwarp();
+        if (size > 32) __syncthreads(); else __syncwarp();
 #endif
     }
     // Exclusive prefix of v over the lanes; *total = the sum (all lanes).
     NE_HD uint32_t scan(uint32_t v, uint32_t& total) const {
 #ifdef __CUDA_ARCH__
+        const int wl = lane & 31;
         uint32_t x = v;
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t t = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += t;
+            if (wl >= o) x += t;
         }
-        total = __shfl_sync(0xffffffffu, x, 31);
-        return x - v;
+        if (size <= 32) {
+            total = __shfl_sync(0xffffffffu, x, 31);
+            return x - v;
+        }
+        const int w = lane >> 5, nw = size >> 5;
+        if (wl == 31) sm[w] = x;
+        __syncthreads();
+        uint32_t before = 0, all = 0;
+        for (int k = 0; k < nw; ++k) {
+            if (k < w) before += sm[k];
+            all += sm[k];
+        }
+        __syncthreads();
+        total = all;
+        return before + x - v;
 #else
         total = v;
         return 0;
@@ -422,17 +440,30 @@ struct Team {
     }
     NE_HD int any_or(int v) const {
 #ifdef __CUDA_ARCH__
+        if (size > 32) return __syncthreads_or(v);
         for (int o = 16; o > 0; o >>= 1) v |= __shfl_xor_sync(0xffffffffu, v, o);
 #endif
         return v;
     }
+    // Sum over the lanes, in a fixed order (warp trees, then warps in order).
     NE_HD double sum(double v) const {
 #ifdef __CUDA_ARCH__
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-#endif
+        if (size <= 32) return v;
+        double* smd = reinterpret_cast<double*>(sm + 32);
+        if ((lane & 31) == 0) smd[lane >> 5] = v;
+        __syncthreads();
+        double r = 0.0;
+        for (int k = 0; k < (size >> 5); ++k) r += smd[k];
+        __syncthreads();
+        return r;
+#else
         return v;
+#endif
     }
 };
+// Shared scratch of a block team: 32 words for the scan, 32 doubles for the sum.
+constexpr int kTeamScratch = 32 + 64;
 
 NE_HD uint32_t uf_root(uint32_t* p, uint32_t x) {
     while (p[x] != x) x = p[x];
