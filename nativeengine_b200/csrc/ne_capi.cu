@@ -89,6 +89,7 @@ struct NeWorld {
     uint32_t big_team_max = 1;
     bool shape_chosen = false;            // set by the caller or the autotuner (else per upload)
     bool has_ext = false;                 // some body is a triangle mesh or a compound
+    bool class_sort = false;              // some world holds two or more non-plane shapes
     size_t nverts = 0;                    // convex vertex pool entries on the device
     uint64_t Rcap = 0;                    // capacity of the recorded pair list
     int key_bits = 64;
@@ -173,6 +174,7 @@ int alloc_rec(NeWorld* w, uint64_t cap) {
 void free_surv_arrays(NeWorld* w) {
     neb::DevWorld& d = w->d;
     dfree(d.si); dfree(d.sj); dfree(d.stage_j); dfree(d.ccnt); dfree(d.coff); dfree(d.cn); dfree(d.cp);
+    dfree(d.sperm);
 }
 
 void free_con_arrays(NeWorld* w) {
@@ -207,7 +209,7 @@ int alloc_surv(NeWorld* w, uint64_t cap) {
     int rc;
     if ((rc = dalloc(&d.si, cap)) || (rc = dalloc(&d.sj, cap)) || (rc = dalloc(&d.stage_j, cap)) ||
         (rc = dalloc(&d.ccnt, cap)) ||
-        (rc = dalloc(&d.coff, cap)) ||
+        (rc = dalloc(&d.coff, cap)) || (rc = dalloc(&d.sperm, cap)) ||
         (rc = dalloc(&d.cn, 4 * cap)) || (rc = dalloc(&d.cp, 4 * cap)))
         return rc;
     w->Scap = cap;
@@ -283,6 +285,7 @@ neb::StepArgs make_args(const NeWorld* w) {
     a.num_sms = w->num_sms;
     a.local_cap = neb::kLocalCap;
     a.any_ext = w->has_ext ? 1 : 0;
+    a.class_sort = w->class_sort ? 1 : 0;
     return a;
 }
 
@@ -738,6 +741,17 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
     w->has_ext = false;
     for (uint32_t i = 0; i < n; ++i)
         if (b->shape[i] == NE_SHAPE_MESH || b->shape[i] == NE_SHAPE_COMPOUND) w->has_ext = true;
+    // A world of one shape (and planes) gives one kind of narrowphase work;
+    // several shapes mix analytic and GJK/EPA pairs in one warp.
+    w->class_sort = false;
+    for (uint32_t k = 0; k < nworlds && !w->class_sort; ++k) {
+        int first = -1;
+        for (uint32_t i = wbegin[k]; i < wbegin[k + 1]; ++i) {
+            if (b->shape[i] == NE_SHAPE_PLANE) continue;
+            if (first < 0) first = b->shape[i];
+            else if (b->shape[i] != first) { w->class_sort = true; break; }
+        }
+    }
 
     std::vector<double> boundR(n);
     std::vector<int> shapes(n);

@@ -110,6 +110,7 @@ struct DevWorld {
     uint32_t *rec_i, *rec_j;       // reference-rule pair list (recorded steps only)
     // narrowphase: the pairs that pass the filters and the cull, sorted by (i, j)
     uint32_t *si, *sj;
+    uint32_t* sperm;         // [S] survivors in narrowphase order: analytic pairs first, then GJK/EPA
     uint32_t *ccnt, *coff;
     D4 *cn, *cp;             // 4 slots per survivor: (normal, depth), (point, -)
     // constraints

@@ -894,6 +894,49 @@ __global__ void __launch_bounds__(kT) k_surv_place(StepArgs a) {
     }
 }
 
+// ---- narrowphase order -------------------------------------------------------
+// Pairs the narrowphase settles analytically (planes, sphere-sphere,
+// sphere-cylinder, capsule-capsule, capsule-sphere: the early returns of
+// detect.hpp:33-77) take far less time than the GJK/EPA pairs.  In worlds
+// that mix shapes, the survivors are visited analytic pairs first, then the
+// rest (each class in pair order), so a warp sees one kind of work.  Every
+// pair still writes its own slot, so the order changes no result.
+__device__ __forceinline__ bool analytic_pair(int sa, int sb) {
+    if (sa == SH_MESH || sa == SH_COMPOUND || sb == SH_MESH || sb == SH_COMPOUND) return false;
+    if (sa == SH_PLANE || sb == SH_PLANE) return true;
+    if (sa == SH_SPHERE && sb == SH_SPHERE) return true;
+    if ((sa == SH_SPHERE && sb == SH_CYLINDER) || (sa == SH_CYLINDER && sb == SH_SPHERE)) return true;
+    if (sa == SH_CAPSULE && (sb == SH_CAPSULE || sb == SH_SPHERE)) return true;
+    if (sa == SH_SPHERE && sb == SH_CAPSULE) return true;
+    return false;
+}
+
+// ccnt (free until the narrowphase) holds 1 for analytic pairs; its scan
+// (into coff, also free until then) ranks them.
+__global__ void __launch_bounds__(kT) k_pair_class(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ctl->S) return;
+    const DevWorld& d = a.d;
+    a.d.ccnt[s] = analytic_pair((int)d.meta[d.si[s]].x, (int)d.meta[d.sj[s]].x) ? 1u : 0u;
+}
+
+__global__ void __launch_bounds__(kT) k_pair_order(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ctl->S) return;
+    const DevWorld& d = a.d;
+    const uint32_t na = (uint32_t)ctl->scan_total;   // analytic pairs
+    const uint32_t r = d.coff[s];                       // analytic pairs before s
+    d.sperm[d.ccnt[s] ? r : na + ((uint32_t)s - r)] = (uint32_t)s;
+}
+
+__device__ __forceinline__ uint64_t narrow_slot(const StepArgs& a, uint64_t t) {
+    return a.class_sort ? (uint64_t)a.d.sperm[t] : t;
+}
+
 // ---- triangle meshes and compounds (src/world.cpp:53-121) --------------------
 // A pair with a mesh or a compound can have any number of contacts: the
 // narrowphase counts them, and once the scan has placed every pair,
@@ -1076,8 +1119,9 @@ __global__ void __launch_bounds__(128) k_narrowphase_ext(StepArgs a) {
 __global__ void __launch_bounds__(128) k_narrowphase(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
-    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= ctl->S) return;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ctl->S) return;
+    const uint64_t s = narrow_slot(a, t);
     const DevWorld& d = a.d;
     const uint32_t i = d.si[s], j = d.sj[s];
     const BodyG A = load_geom(d, i), B = load_geom(d, j);
@@ -1663,6 +1707,11 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
         k_surv_gather<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a, kb); ++L;
         scan_u32(d.bcnt, d.boff, a.n, d.tsum, &ctl->S, ctl, st, launches);
         k_surv_place<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a); ++L;
+    }
+    if (a.class_sort) {
+        k_pair_class<<<blocks_for(a.Scap, kT), kT, 0, st>>>(a); ++L;
+        scan_u32(d.ccnt, d.coff, (uint32_t)a.Scap, d.tsum, &ctl->scan_total, ctl, st, launches, &ctl->S);
+        k_pair_order<<<blocks_for(a.Scap, kT), kT, 0, st>>>(a); ++L;
     }
     mark(3);
     if (a.f32) {

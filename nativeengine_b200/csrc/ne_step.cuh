@@ -52,6 +52,7 @@ struct StepArgs {
     int sticky;              // replayed batch: an aborted step halts the rest of the batch
     uint32_t local_cap;      // big islands up to this many contacts: shared-memory dataflow solver
     int any_ext;             // some body is a triangle mesh or a compound (second narrowphase pass)
+    int class_sort;          // some world mixes shapes: narrowphase in class order (d.sperm)
 };
 
 // Contacts per island the shared-memory dataflow solver takes (one counter

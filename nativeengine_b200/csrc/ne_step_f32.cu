@@ -60,8 +60,9 @@ __device__ __forceinline__ BodyGT<float> load_geom_f32(const DevWorld& d, uint32
 __global__ void __launch_bounds__(128) k_narrowphase_f32(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
-    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= ctl->S) return;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ctl->S) return;
+    const uint64_t s = a.class_sort ? (uint64_t)a.d.sperm[t] : t;   // narrowphase order (ne_step.cu)
     const DevWorld& d = a.d;
     const uint32_t i = d.si[s], j = d.sj[s];
     // Triangle meshes and compounds: their contacts come from the FP64
