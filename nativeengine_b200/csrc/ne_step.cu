@@ -5,11 +5,16 @@
 //   broadphasePairs()      src/world.cpp:424-501   k_cell_keys, radix sort, cell table (k_cell_flags,
 //                                                  k_cell_table); reference-rule list: k_pair_count, k_pair_emit
 //   pair filters + cull    src/world.cpp:513-516   k_surv_gather, k_surv_place (fused with the pair lists)
-//   gatherContacts()       src/world.cpp:88-130    k_narrowphase (ne_geom.cuh)
+//   gatherContacts()       src/world.cpp:88-130    k_narrowphase (ne_geom.cuh), in class order when
+//                                                  worlds mix shapes (k_pair_class, k_pair_order);
+//                                                  meshes and compounds: k_narrowphase_ext
 //   constraint build       src/world.cpp:537-553   k_constraint_build (+ union-find hooking)
-//   islands                src/world.cpp:332-343   k_island_label, radix sort, k_island_mark/_start
+//   islands                src/world.cpp:332-343   k_island_label, radix sort, k_island_mark/_start,
+//                                                  k_island_list
 //   warm start + 8 SI + position correction + warm-cache store
-//                          src/world.cpp:559-626   k_island_solve, k_island_solve_big
+//                          src/world.cpp:559-626   k_island_solve (small islands, side stream),
+//                                                  k_big_rec + k_island_solve_shared (big islands),
+//                                                  k_island_solve_local / k_island_solve_big
 //   wrapPositions/applyWalls src/world.cpp:635-702 k_boundary
 //
 // Every kernel is a no-op once ctl->abort is set (a capacity overflow this
