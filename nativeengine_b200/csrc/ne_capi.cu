@@ -192,7 +192,7 @@ int alloc_scratch(NeWorld* w) {
     neb::DevWorld& d = w->d;
     dfree(d.hist);
     dfree(d.tsum);
-    uint64_t sortn = std::max<uint64_t>(w->n, 2 * w->Ccap);
+    uint64_t sortn = std::max<uint64_t>(std::max<uint64_t>(w->n, 2 * w->Ccap), w->Scap);
     size_t hw = neb::radix_hist_words((uint32_t)sortn);
     uint64_t scann = std::max<uint64_t>(w->Scap, std::max<uint64_t>(hw, sortn));
     int rc;

@@ -6,7 +6,7 @@
 //                                                  k_cell_table); reference-rule list: k_pair_count, k_pair_emit
 //   pair filters + cull    src/world.cpp:513-516   k_surv_gather, k_surv_place (fused with the pair lists)
 //   gatherContacts()       src/world.cpp:88-130    k_narrowphase (ne_geom.cuh), in class order when
-//                                                  worlds mix shapes (k_pair_class, k_pair_order);
+//                                                  worlds mix shapes (k_pair_class + a radix sort);
 //                                                  meshes and compounds: k_narrowphase_ext
 //   constraint build       src/world.cpp:537-553   k_constraint_build (+ union-find hooking)
 //   islands                src/world.cpp:332-343   k_island_label, radix sort, k_island_mark/_start,
@@ -900,42 +900,27 @@ __global__ void __launch_bounds__(kT) k_surv_place(StepArgs a) {
 }
 
 // ---- narrowphase order -------------------------------------------------------
-// Pairs the narrowphase settles analytically (planes, sphere-sphere,
-// sphere-cylinder, capsule-capsule, capsule-sphere: the early returns of
-// detect.hpp:33-77) take far less time than the GJK/EPA pairs.  In worlds
-// that mix shapes, the survivors are visited analytic pairs first, then the
-// rest (each class in pair order), so a warp sees one kind of work.  Every
-// pair still writes its own slot, so the order changes no result.
-__device__ __forceinline__ bool analytic_pair(int sa, int sb) {
-    if (sa == SH_MESH || sa == SH_COMPOUND || sb == SH_MESH || sb == SH_COMPOUND) return false;
-    if (sa == SH_PLANE || sb == SH_PLANE) return true;
-    if (sa == SH_SPHERE && sb == SH_SPHERE) return true;
-    if ((sa == SH_SPHERE && sb == SH_CYLINDER) || (sa == SH_CYLINDER && sb == SH_SPHERE)) return true;
-    if (sa == SH_CAPSULE && (sb == SH_CAPSULE || sb == SH_SPHERE)) return true;
-    if (sa == SH_SPHERE && sb == SH_CAPSULE) return true;
-    return false;
+// In worlds that mix shapes, neighbouring pairs take different narrowphase
+// paths (the analytic early returns of detect.hpp:33-77, or GJK/EPA with
+// different support functions), and a warp waits for its slowest lane.  There
+// the survivors are visited grouped by shape pair: a stable one-pass radix sort
+// on the pair's shape code keeps pair order inside each group.  Every pair
+// still writes its own slot, so the order changes no result.
+__device__ __forceinline__ uint32_t shape_pair_code(int sa, int sb) {
+    const int lo = sa < sb ? sa : sb, hi = sa < sb ? sb : sa;
+    return (uint32_t)(lo * 8 + hi);   // 0..63
 }
 
-// ccnt (free until the narrowphase) holds 1 for analytic pairs; its scan
-// (into coff, also free until then) ranks them.
+// Keys (ccnt, free until the narrowphase) and identity values (stage_j,
+// free after the placement) for the sort into sperm.
 __global__ void __launch_bounds__(kT) k_pair_class(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= ctl->S) return;
     const DevWorld& d = a.d;
-    a.d.ccnt[s] = analytic_pair((int)d.meta[d.si[s]].x, (int)d.meta[d.sj[s]].x) ? 1u : 0u;
-}
-
-__global__ void __launch_bounds__(kT) k_pair_order(StepArgs a) {
-    Ctl* ctl = a.d.ctl;
-    if (ctl->abort) return;
-    const uint64_t s = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= ctl->S) return;
-    const DevWorld& d = a.d;
-    const uint32_t na = (uint32_t)ctl->scan_total;   // analytic pairs
-    const uint32_t r = d.coff[s];                       // analytic pairs before s
-    d.sperm[d.ccnt[s] ? r : na + ((uint32_t)s - r)] = (uint32_t)s;
+    d.ccnt[s] = shape_pair_code((int)d.meta[d.si[s]].x, (int)d.meta[d.sj[s]].x);
+    d.stage_j[s] = (uint32_t)s;
 }
 
 __device__ __forceinline__ uint64_t narrow_slot(const StepArgs& a, uint64_t t) {
@@ -1715,8 +1700,10 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
     }
     if (a.class_sort) {
         k_pair_class<<<blocks_for(a.Scap, kT), kT, 0, st>>>(a); ++L;
-        scan_u32(d.ccnt, d.coff, (uint32_t)a.Scap, d.tsum, &ctl->scan_total, ctl, st, launches, &ctl->S);
-        k_pair_order<<<blocks_for(a.Scap, kT), kT, 0, st>>>(a); ++L;
+        // 6-bit keys: one pass, so the values end in buffer 1 (sperm).
+        uint32_t* pk[2] = {d.ccnt, d.coff};
+        uint32_t* pv[2] = {d.stage_j, d.sperm};
+        radix_sort_u32(pk, pv, (uint32_t)a.Scap, 6, d.hist, d.tsum, ctl, st, launches, &ctl->S);
     }
     mark(3);
     if (a.f32) {
