@@ -66,6 +66,7 @@ struct NeWorld {
     int device = 0;
     cudaStream_t stream = nullptr;
     neb::SideStream side{};               // small-island solve beside the big-island solvers
+    cudaEvent_t dl_ev[6] = {};            // per-array completion of a state download
     uint32_t n = 0;
     neb::DevWorld d{};
     neb::Ctl* h_ctl = nullptr;   // pinned mirror of d.ctl
@@ -473,6 +474,7 @@ int ne_world_create(const NeWorldParams* params, NeWorld** out) {
     NE_CUDA_TRY(cudaStreamCreateWithFlags(&w->side.st2, cudaStreamNonBlocking));
     NE_CUDA_TRY(cudaEventCreateWithFlags(&w->side.fork, cudaEventDisableTiming));
     NE_CUDA_TRY(cudaEventCreateWithFlags(&w->side.join, cudaEventDisableTiming));
+    for (int k = 0; k < 6; ++k) NE_CUDA_TRY(cudaEventCreateWithFlags(&w->dl_ev[k], cudaEventDisableTiming));
     neb::init_kernel_attrs();
     NE_CUDA_TRY(cudaGetLastError());
     NE_CUDA_TRY(cudaMallocHost((void**)&w->h_ctl, sizeof(neb::Ctl)));
@@ -504,6 +506,8 @@ int ne_world_destroy(NeWorld* w) {
     if (w->side.st2) cudaStreamSynchronize(w->side.st2);
     if (w->side.fork) cudaEventDestroy(w->side.fork);
     if (w->side.join) cudaEventDestroy(w->side.join);
+    for (int k = 0; k < 6; ++k)
+        if (w->dl_ev[k]) cudaEventDestroy(w->dl_ev[k]);
     if (w->side.st2) cudaStreamDestroy(w->side.st2);
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
@@ -1053,11 +1057,13 @@ static int ensure_io(NeWorld* w) {
     return NE_OK;
 }
 
-// memcpy split over a few threads: one thread does not saturate the host
-// memory bandwidth for the ~100 MB a large batch moves per step.
+// memcpy split over up to 16 threads (at least 1 MiB each): one thread does
+// not saturate the host memory bandwidth for the ~100 MB a large batch moves
+// per step.
 static void par_copy(void* dst, const void* src, size_t bytes) {
-    const size_t kChunk = (size_t)8 << 20;
-    const unsigned nt = (unsigned)std::min<size_t>(8, bytes / kChunk);
+    const size_t kChunk = (size_t)1 << 20;
+    const size_t hw = std::max<size_t>(1, std::thread::hardware_concurrency());
+    const unsigned nt = (unsigned)std::min<size_t>(std::min<size_t>(16, hw), bytes / kChunk);
     if (nt < 2) {
         std::memcpy(dst, src, bytes);
         return;
@@ -1085,13 +1091,15 @@ int ne_world_upload_state(NeWorld* w, const double* x, const double* q, const do
     const size_t off[4] = {0, 3 * N, 7 * N, 10 * N};
     const size_t len[4] = {3 * N, 4 * N, 3 * N, 3 * N};
     uint32_t mask = 0;
+    // Array by array: the transfer of one overlaps the staging copy of the next.
     for (int k = 0; k < 4; ++k) {
         if (!src[k]) continue;
         par_copy(st + off[k], src[k], len[k] * sizeof(double));
+        NE_CUDA_TRY(cudaMemcpyAsync(w->d.io + off[k], st + off[k], len[k] * sizeof(double),
+                                    cudaMemcpyHostToDevice, w->stream));
         mask |= 1u << k;
     }
     if (!mask) return NE_OK;
-    NE_CUDA_TRY(cudaMemcpyAsync(w->d.io, st, 13 * N * sizeof(double), cudaMemcpyHostToDevice, w->stream));
     neb::launch_unpack_state(w->d, n, w->d.io, mask, w->stream);
     NE_CUDA_TRY(cudaGetLastError());
     // The staging buffer is reused by the next call: wait for the copy.
@@ -1112,17 +1120,24 @@ int ne_world_download(NeWorld* w, NeBodyArrays* out) {
     const size_t off[6] = {0, 3 * N, 7 * N, 10 * N, 13 * N, 16 * N};
     const size_t per[6] = {3, 4, 3, 3, 3, 3};
     uint32_t mask = 0;
-    size_t end = 0;
     for (int k = 0; k < 6; ++k)
-        if (dst[k]) { mask |= 1u << k; end = off[k] + per[k] * N; }
+        if (dst[k]) mask |= 1u << k;
     if (!mask) return NE_OK;
     neb::launch_pack_state(w->d, w->n, w->d.io, mask, w->stream);
     NE_CUDA_TRY(cudaGetLastError());
     double* st = w->pinned;
-    NE_CUDA_TRY(cudaMemcpyAsync(st, w->d.io, end * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
-    NE_CUDA_TRY(cudaStreamSynchronize(w->stream));
-    for (int k = 0; k < 6; ++k)
-        if (dst[k]) par_copy(dst[k], st + off[k], per[k] * (size_t)n * sizeof(double));
+    // Array by array: the copy out of one overlaps the transfer of the next.
+    for (int k = 0; k < 6; ++k) {
+        if (!dst[k]) continue;
+        NE_CUDA_TRY(cudaMemcpyAsync(st + off[k], w->d.io + off[k], per[k] * N * sizeof(double),
+                                    cudaMemcpyDeviceToHost, w->stream));
+        NE_CUDA_TRY(cudaEventRecord(w->dl_ev[k], w->stream));
+    }
+    for (int k = 0; k < 6; ++k) {
+        if (!dst[k]) continue;
+        NE_CUDA_TRY(cudaEventSynchronize(w->dl_ev[k]));
+        par_copy(dst[k], st + off[k], per[k] * (size_t)n * sizeof(double));
+    }
     return NE_OK;
 }
 
