@@ -506,8 +506,9 @@ def run_ours(args):
                          "peak_source": peak_kind, "traffic": profile_traffic(C_last),
                          "note": "latency-bound: the exact Gauss-Seidel order is a dependency chain; "
                                  "algorithmic bytes = 144 B/contact + 200 B/body of the last step"},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * 32 * work,
-                    "d2h_bytes_per_step": 4 * 32 * work},
+            # x, q, v, w: 13 doubles per body each way (ne_world_upload_state / ne_world_download)
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 13 * 8 * work,
+                    "d2h_bytes_per_step": 13 * 8 * work},
             "gpu_launches": launches,
             "clocks": clocks,
             "stage_ms_per_step": stage_ms,
