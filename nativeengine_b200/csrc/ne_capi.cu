@@ -128,7 +128,9 @@ void free_body_arrays(NeWorld* w) {
     dfree(d.key[0]); dfree(d.key[1]); dfree(d.val[0]); dfree(d.val[1]);
     dfree(d.bcnt); dfree(d.boff); dfree(d.parent); dfree(d.bdeg); dfree(d.bstart);
     dfree(d.cflag); dfree(d.crun); dfree(d.cstart); dfree(d.hkey); dfree(d.hval); dfree(d.bstage); dfree(d.srec);
+    dfree(d.lrow); dfree(d.lmask);
     d.hsize = 0;
+    d.lwords = 0;
     dfree(d.f_v); dfree(d.f_w); dfree(d.f_q); dfree(d.f_I); dfree(d.f_e); dfree(d.f_verts);
 }
 
@@ -709,6 +711,9 @@ int upload_impl(NeWorld* w, const NeWorldParams* params, uint32_t nworlds, const
         while (hs < 2 * m) hs <<= 1;
         if ((rc = dalloc(&d.hkey, hs)) || (rc = dalloc(&d.hval, hs))) return rc;
         d.hsize = hs;
+        const size_t lw = (m + 31) / 32 + 1;
+        if ((rc = dalloc(&d.lrow, neb::kLongRows)) || (rc = dalloc(&d.lmask, neb::kLongRows * lw))) return rc;
+        d.lwords = (uint32_t)lw;
     }
     // Pack the host arrays into the 32-byte device records.
     std::vector<neb::D4>& st = w->stage;

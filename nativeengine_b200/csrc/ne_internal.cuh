@@ -68,12 +68,18 @@ struct Ctl {
     uint32_t big_class[32];
     uint32_t big_fill[32];
     uint32_t big_next;
-    uint32_t pad2_;
+    uint32_t nlong;          // long partner lists split over many warps this step
 };
 
 // Islands with at least kBigIsland contacts go to the team (dataflow)
 // solver; smaller ones are solved one thread per island.
 constexpr uint32_t kBigIsland = 48;
+
+// Partner lists of at least kLongRow candidates are culled by many warps
+// (k_long_mask, k_long_place); up to kLongRows of them per step, the rest on
+// one warp each like every other list.
+constexpr uint32_t kLongRow = 512;
+constexpr uint32_t kLongRows = 64;
 
 // Big-island solver control block: ready-queue head (claims) and tail
 // (pushes), updates done, failure flag.
@@ -106,6 +112,11 @@ struct DevWorld {
     uint32_t* hval;                    // [hsize]
     uint32_t hsize;                    // power of two >= 2n
     uint32_t *stage_j, *bstage;        // [Scap] staged partner lists, [n] staging offset per body
+    // long partner lists (every later body of the world: brute-force worlds
+    // and grid-excluded bodies): the body of each slot and one keep bit per
+    // candidate, lwords words per slot
+    uint32_t *lrow, *lmask;            // [kLongRows], [kLongRows * lwords]
+    uint32_t lwords;                   // ceil(n / 32) + 1
     D4* srec;                          // [n] (x, y, z, boundR) in sorted cell order
     uint32_t *rec_i, *rec_j;       // reference-rule pair list (recorded steps only)
     // narrowphase: the pairs that pass the filters and the cull, sorted by (i, j)

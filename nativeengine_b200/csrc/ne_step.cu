@@ -237,6 +237,7 @@ __global__ void k_step_begin(Ctl* ctl, int sticky) {
     ctl->nbig = 0;
     for (int k = 0; k < 32; ++k) ctl->big_class[k] = ctl->big_fill[k] = 0;
     ctl->big_next = 0;
+    ctl->nlong = 0;
     ctl->solve_timeout = 0;
     ctl->S_stage = 0;
 }
@@ -772,6 +773,7 @@ __global__ void __launch_bounds__(kT, 5) k_surv_gather(StepArgs a, int kb) {
     CullA A;
     GridSel G;
     uint32_t wend = 0;
+    bool split = false;
     if (i < a.n) {
         const uint32_t w = a.bw[i];
         const WorldP& W = a.wp[w];
@@ -780,7 +782,16 @@ __global__ void __launch_bounds__(kT, 5) k_surv_gather(StepArgs a, int kb) {
         wend = W.end;
         if (G.brute || excluded(A.m, 1)) {
             cand = W.end - 1 - i;
-            for (uint32_t j0 = i + 1; j0 < W.end; j0 += 32) {
+            if (cand >= kLongRow) {
+                uint32_t slot = 0;
+                if (lane == 0) slot = atomicAdd(&ctl->nlong, 1u);
+                slot = __shfl_sync(0xffffffffu, slot, 0);
+                if (slot < kLongRows) {
+                    if (lane == 0) d.lrow[slot] = i;
+                    split = true;   // k_long_mask / k_long_place take this list
+                }
+            }
+            for (uint32_t j0 = i + 1; !split && j0 < W.end; j0 += 32) {
                 const uint32_t j = j0 + lane;
                 const bool k = j < W.end && cull_keep(d, A, j);
                 const uint32_t bal = __ballot_sync(0xffffffffu, k);
@@ -870,9 +881,93 @@ __global__ void __launch_bounds__(kT, 5) k_surv_gather(StepArgs a, int kb) {
             }
         }
     }
-    if (lane == 0) {
+    if (lane == 0 && !split) {
         d.bcnt[i] = cnt;
         d.bstage[i] = off;
+    }
+}
+
+// Long partner lists (every later body of the world) split over the warps of
+// the whole grid: one warp per 32 candidates writes their keep bits
+// (cull_keep, the test of the one-warp walk) as one mask word.
+__global__ void __launch_bounds__(kT) k_long_mask(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint32_t nl = min(ctl->nlong, kLongRows);
+    if (nl == 0) return;
+    const int lane = threadIdx.x & 31;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const DevWorld& d = a.d;
+    for (uint32_t slot = 0; slot < nl; ++slot) {
+        const uint32_t i = d.lrow[slot];
+        const uint32_t wend = a.wp[a.bw[i]].end;
+        const uint32_t nw = (wend - 1 - i + 31) / 32;
+        if (warp >= nw) continue;
+        const CullA A = cull_self(a, i);
+        for (uint32_t c = warp; c < nw; c += nwarps) {
+            const uint32_t j = i + 1 + c * 32 + lane;
+            const bool k = j < wend && cull_keep(d, A, j);
+            const uint32_t bal = __ballot_sync(0xffffffffu, k);
+            if (lane == 0) d.lmask[(size_t)slot * d.lwords + c] = bal;
+        }
+    }
+}
+
+// The survivors of each long list, ascending, at one staging reservation:
+// one block per list; a block-wide scan of the mask words' bit counts places
+// every survivor.  Sets the list's bcnt / bstage like k_surv_gather.
+constexpr int kPlaceT = 512;
+__global__ void __launch_bounds__(kPlaceT) k_long_place(StepArgs a) {
+    Ctl* ctl = a.d.ctl;
+    if (ctl->abort) return;
+    const uint32_t slot = blockIdx.x;
+    if (slot >= min(ctl->nlong, kLongRows)) return;
+    __shared__ uint32_t s_w[kPlaceT / 32];
+    __shared__ uint32_t s_base, s_tile;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const DevWorld& d = a.d;
+    const uint32_t i = d.lrow[slot];
+    const uint32_t wend = a.wp[a.bw[i]].end;
+    const uint32_t nw = (wend - 1 - i + 31) / 32;
+    const uint32_t* mask = d.lmask + (size_t)slot * d.lwords;
+    uint32_t cnt = 0;
+    for (uint32_t c = threadIdx.x; c < nw; c += kPlaceT) cnt += __popc(mask[c]);
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if (lane == 0) s_w[wid] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int k = 0; k < kPlaceT / 32; ++k) tot += s_w[k];
+        const uint32_t off = tot ? (uint32_t)atomicAdd((unsigned long long*)&ctl->S_stage, (unsigned long long)tot) : 0u;
+        d.bcnt[i] = tot;
+        d.bstage[i] = off;
+        s_base = off;
+        s_tile = 0;
+    }
+    __syncthreads();
+    for (uint32_t c0 = 0; c0 < nw; c0 += kPlaceT) {
+        const uint32_t c = c0 + threadIdx.x;
+        const uint32_t m = c < nw ? mask[c] : 0u;
+        const uint32_t pc = __popc(m);
+        uint32_t incl = pc;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) s_w[wid] = incl;
+        __syncthreads();
+        uint32_t before = s_tile;
+        for (int k = 0; k < wid; ++k) before += s_w[k];
+        uint32_t pos = s_base + before + incl - pc;
+        for (uint32_t b = m; b; b &= b - 1u) {
+            const uint32_t j = i + 1 + c * 32 + (uint32_t)__ffs(b) - 1u;
+            if ((uint64_t)pos < a.Scap) d.stage_j[pos] = j;
+            ++pos;
+        }
+        __syncthreads();
+        if (threadIdx.x == kPlaceT - 1) s_tile = before + incl;
+        __syncthreads();
     }
 }
 
@@ -1695,6 +1790,12 @@ void launch_step(const StepArgs& a0, cudaStream_t st, uint64_t* launches, cudaEv
         }
         mark(2);
         k_surv_gather<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a, kb); ++L;
+        {
+            // one warp per 32 candidates of the longest possible list, at most 2 blocks per SM
+            const uint32_t lb = (uint32_t)std::min<uint64_t>(((uint64_t)a.n + 32 * (kT / 32) - 1) / (32 * (kT / 32)), 296);
+            k_long_mask<<<lb ? lb : 1, kT, 0, st>>>(a); ++L;
+            k_long_place<<<kLongRows, kPlaceT, 0, st>>>(a); ++L;
+        }
         scan_u32(d.bcnt, d.boff, a.n, d.tsum, &ctl->S, ctl, st, launches);
         k_surv_place<<<blocks_for((uint64_t)a.n * 32, kT), kT, 0, st>>>(a); ++L;
     }

@@ -109,3 +109,33 @@ def test_device_epa_stays_bounded():
         assert rc in (_ffi.NE_OK, _ffi.NE_ERR_NUMERIC)
     st = dev.state()
     assert all(np.isfinite(st[k]).all() for k in ("x", "q", "v", "w"))
+
+
+def _long_lists(brute):
+    """Piles whose partner lists reach every later body of the world: the
+    ground box's list (577 bodies) and, under forced brute force, the first
+    ~200 lists of 721 bodies -- more long lists than the device splits per
+    step, so the rest take the one-warp walk."""
+    if brute:
+        params, bodies = scenes.box_pile(8, 9, 10, seed=6)
+        params.force_brute_force = 1
+        return params, bodies
+    return scenes.box_pile(8, 8, 9, seed=7)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("brute", [False, True])
+def test_long_partner_lists_match_the_oracle(brute, oracle_cls):
+    params, bodies = _long_lists(brute)
+    dev = DeviceWorld(params, bodies.copy())
+    ora = oracle_cls(params, bodies.copy())
+    for s in range(90):
+        dev.step(1)
+        ora.step(1)
+        if s % 15 == 14:
+            what = f"brute={brute} step {s}"
+            assert_same_pairs(dev, ora, what)
+            assert_same_contacts(dev, ora, 0.0, what)
+            assert_same_state(dev, ora, 0.0, what)
+    assert dev.stats()["contacts"] > 0
+    dev.close()
