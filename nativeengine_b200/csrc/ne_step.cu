@@ -888,29 +888,46 @@ __global__ void __launch_bounds__(kT, 5) k_surv_gather(StepArgs a, int kb) {
 }
 
 // Long partner lists (every later body of the world) split over the warps of
-// the whole grid: one warp per 32 candidates writes their keep bits
+// the whole grid: the lists' 32-candidate chunks are numbered through in slot
+// order, and each warp takes every nwarps-th chunk and writes its keep bits
 // (cull_keep, the test of the one-warp walk) as one mask word.
 __global__ void __launch_bounds__(kT) k_long_mask(StepArgs a) {
     Ctl* ctl = a.d.ctl;
     if (ctl->abort) return;
     const uint32_t nl = min(ctl->nlong, kLongRows);
     if (nl == 0) return;
+    __shared__ uint32_t s_i[kLongRows], s_end[kLongRows], s_pre[kLongRows + 1];
+    const DevWorld& d = a.d;
+    if (threadIdx.x < nl) {
+        const uint32_t i = d.lrow[threadIdx.x];
+        s_i[threadIdx.x] = i;
+        s_end[threadIdx.x] = a.wp[a.bw[i]].end;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for (uint32_t k = 0; k < nl; ++k) {
+            s_pre[k] = acc;
+            acc += (s_end[k] - 1 - s_i[k] + 31) / 32;
+        }
+        s_pre[nl] = acc;
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    const DevWorld& d = a.d;
-    for (uint32_t slot = 0; slot < nl; ++slot) {
-        const uint32_t i = d.lrow[slot];
-        const uint32_t wend = a.wp[a.bw[i]].end;
-        const uint32_t nw = (wend - 1 - i + 31) / 32;
-        if (warp >= nw) continue;
-        const CullA A = cull_self(a, i);
-        for (uint32_t c = warp; c < nw; c += nwarps) {
-            const uint32_t j = i + 1 + c * 32 + lane;
-            const bool k = j < wend && cull_keep(d, A, j);
-            const uint32_t bal = __ballot_sync(0xffffffffu, k);
-            if (lane == 0) d.lmask[(size_t)slot * d.lwords + c] = bal;
+    for (uint32_t g = warp; g < s_pre[nl]; g += nwarps) {
+        uint32_t lo = 0, hi = nl - 1;   // the slot whose chunks hold g
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if (s_pre[mid] <= g) lo = mid; else hi = mid - 1;
         }
+        const uint32_t i = s_i[lo], wend = s_end[lo], c = g - s_pre[lo];
+        const CullA A = cull_self(a, i);
+        const uint32_t j = i + 1 + c * 32 + lane;
+        const bool k = j < wend && cull_keep(d, A, j);
+        const uint32_t bal = __ballot_sync(0xffffffffu, k);
+        if (lane == 0) d.lmask[(size_t)lo * d.lwords + c] = bal;
     }
 }
 
